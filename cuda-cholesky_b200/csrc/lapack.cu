@@ -1,0 +1,617 @@
+// Host drivers of the dense SPD path and the C ABI of include/lapack.h.
+//
+// All four element types run the same drivers (templates over T).  Upper storage
+// is handled by running the lower algorithm on the transposed view of A (element
+// (i, j) of the logical lower triangle at A[i*rs + j*cs], (rs, cs) = (lda, 1)), which
+// produces U = L^T in place; see diag.cuh.
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "diag.cuh"
+#include "gemm.cuh"
+#include "handle.h"
+
+using namespace cuchol;
+
+// ------------------------------------------------------------------------------
+// Hooks (reference blas/xerbla.c:5-9, multigpu/error.c:4-11)
+// ------------------------------------------------------------------------------
+static void default_xerbla(const char* function, long info) {
+  fprintf(stderr, "On entry to %s parameter %ld had an invalid value\n", function, info);
+}
+static void default_error_handler(const char* call, const char* function, const char* file, int line,
+                                  int error, const char* (*strerror)(int)) {
+  fprintf(stderr, "Error:\n\t%s returned %d (%s) in %s (%s:%d)\n", call, error, strerror(error), function,
+          file, line);
+}
+#define CUCHOL_EXPORT __attribute__((visibility("default")))
+extern "C" {
+CUCHOL_EXPORT xerbla_t xerbla = &default_xerbla;
+CUCHOL_EXPORT errorHandler_t errorHandler = &default_error_handler;
+}
+
+namespace cuchol {
+
+const char* error_string(int e) { return cudaGetErrorString(static_cast<cudaError_t>(e)); }
+
+CUresult report(cudaError_t e, const char* call, const char* func, const char* file, int line) {
+  if (errorHandler != nullptr) errorHandler(call, func, file, line, (int)e, &error_string);
+  return to_cu(e);
+}
+
+CUresult ensure_workspace(CULAPACKhandle h, size_t bytes) {
+  if (bytes <= h->ws_bytes) return CUDA_SUCCESS;
+  CUCHOL_CHECK(cudaStreamSynchronize(h->s_panel));
+  CUCHOL_CHECK(cudaStreamSynchronize(h->s_update));
+  if (h->ws != nullptr) CUCHOL_CHECK(cudaFree(h->ws));
+  h->ws = nullptr;
+  h->ws_bytes = 0;
+  CUCHOL_CHECK(cudaMalloc(&h->ws, bytes));
+  h->ws_bytes = bytes;
+  return CUDA_SUCCESS;
+}
+
+void* stage_descriptors(CULAPACKhandle h, const void* src, size_t bytes, cudaStream_t s) {
+  size_t off = (h->desc_used + 255) & ~size_t(255);
+  if (off + bytes > h->desc_bytes) return nullptr;
+  memcpy(static_cast<char*>(h->desc_host) + off, src, bytes);
+  void* dst = static_cast<char*>(h->desc_dev) + off;
+  if (cudaMemcpyAsync(dst, static_cast<char*>(h->desc_host) + off, bytes, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return nullptr;
+  h->desc_used = off + bytes;
+  return dst;
+}
+
+}  // namespace cuchol
+
+namespace {
+
+__global__ void narrow_double_kernel(const double* s, float* d) { *d = (float)*s; }
+
+constexpr int kDiagThreads = 512;
+
+template <typename T> struct Tune { static constexpr int nb = 128; };
+template <> struct Tune<cuDoubleComplex> { static constexpr int nb = 64; };
+
+inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ---- tile engine launcher -------------------------------------------------------
+template <typename T, int LA, int LB>
+CUresult launch_simt(CULAPACKhandle h, const GemmLaunch<T>& L, int tiles, cudaStream_t s, const int* abort) {
+  gemm_simt_kernel<T, LA, LB><<<tiles, 256, 0, s>>>(L, abort);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+template <typename T>
+CUresult launch_dispatch(CULAPACKhandle h, const GemmLaunch<T>& L, int tiles, int la, int lb, cudaStream_t s,
+                         const int* abort) {
+  if (la == 0 && lb == 0) return launch_simt<T, 0, 0>(h, L, tiles, s, abort);
+  if (la == 0 && lb == 1) return launch_simt<T, 0, 1>(h, L, tiles, s, abort);
+  if (la == 1 && lb == 0) return launch_simt<T, 1, 0>(h, L, tiles, s, abort);
+  return launch_simt<T, 1, 1>(h, L, tiles, s, abort);
+}
+
+constexpr int kTile = 64;
+
+template <typename T>
+CUresult gemm(CULAPACKhandle h, GemmProblem<T> p, cudaStream_t s, const int* abort) {
+  if (p.m <= 0 || p.n <= 0) return CUDA_SUCCESS;
+  p.tiles_n = (p.n + kTile - 1) / kTile;
+  p.tile_begin = 0;
+  const int tiles = ((p.m + kTile - 1) / kTile) * p.tiles_n;
+  GemmLaunch<T> L{};
+  L.single = p;
+  L.list = nullptr;
+  L.nlist = 0;
+  return launch_dispatch<T>(h, L, tiles, p.a_rs == 1 ? 0 : 1, p.b_rs == 1 ? 0 : 1, s, abort);
+}
+
+// All problems must share the contiguity of their views.
+template <typename T>
+CUresult gemm_group(CULAPACKhandle h, std::vector<GemmProblem<T>>& ps, cudaStream_t s, const int* abort) {
+  if (ps.empty()) return CUDA_SUCCESS;
+  int tiles = 0;
+  for (auto& p : ps) {
+    p.tiles_n = (p.n + kTile - 1) / kTile;
+    p.tile_begin = tiles;
+    tiles += ((p.m + kTile - 1) / kTile) * p.tiles_n;
+  }
+  if (ps.size() == 1) return gemm<T>(h, ps[0], s, abort);
+  void* dev = stage_descriptors(h, ps.data(), ps.size() * sizeof(GemmProblem<T>), s);
+  if (dev == nullptr) {   // list area full: one launch per problem
+    for (auto& p : ps) CUCHOL_CHECK_CU(gemm<T>(h, p, s, abort));
+    return CUDA_SUCCESS;
+  }
+  GemmLaunch<T> L{};
+  L.list = static_cast<const GemmProblem<T>*>(dev);
+  L.nlist = (int)ps.size();
+  return launch_dispatch<T>(h, L, tiles, ps[0].a_rs == 1 ? 0 : 1, ps[0].b_rs == 1 ? 0 : 1, s, abort);
+}
+
+template <typename T>
+GemmProblem<T> problem() {
+  GemmProblem<T> p;
+  memset(&p, 0, sizeof(p));
+  p.alpha = from_real<T>(RealOf<T>(1));
+  p.beta = zero<T>();
+  return p;
+}
+
+template <typename T>
+CUresult copy_view(CULAPACKhandle h, const T* src, long long s_rs, long long s_cs, T* dst, long long d_rs, long long d_cs, int m,
+                   int n, bool lower_only, cudaStream_t s, const int* abort) {
+  if (m <= 0 || n <= 0) return CUDA_SUCCESS;
+  dim3 grid((m + 31) / 32, (n + 31) / 32);
+  copy_view_kernel<T><<<grid, 256, 0, s>>>(src, s_rs, s_cs, dst, d_rs, d_cs, m, n, lower_only ? 1 : 0, abort);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+template <typename T>
+CUresult set_smem(const void* fn, size_t bytes) {
+  CUCHOL_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return CUDA_SUCCESS;
+}
+
+// ---- ?POTRF ---------------------------------------------------------------------
+// Right-looking blocked Cholesky with lookahead depth 1, on two streams:
+//   panel stream : diagonal block (factor + inverse)  -> panel solve into P
+//                  -> copy P into A -> [wait trailing update of the previous step]
+//                  -> update of the next block column (lookahead)
+//   update stream: [wait panel] -> update of the rest of the trailing matrix
+// so the next diagonal block and panel are factored while the previous trailing
+// update is still running.  P is a ping-pong pair of packed panel buffers.
+// Failure: the diagonal-block kernel sets the device info word, and every later
+// kernel exits at entry when it is set.
+template <typename T>
+CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out) {
+  const int nb = Tune<T>::nb;
+  const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
+  auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
+  cudaStream_t sp = h->s_panel, su = h->s_update;
+  int* d_info = h->d_words;
+
+  const long long ldp = (long long)round_up((size_t)n, 2);
+  const size_t ws = sizeof(T) * ((size_t)nb * nb + 2 * (size_t)ldp * nb);
+  CUCHOL_CHECK_CU(ensure_workspace(h, ws));
+  T* winv = static_cast<T*>(h->ws);
+  T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * nb};
+
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)potf2_block_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
+  CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
+  CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
+  // the update stream starts after the panel stream's initialisation
+  CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+  CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+
+  for (int j = 0, step = 0; j < n; j += nb, ++step) {
+    const int jb = std::min(nb, n - j);
+    const int m = n - j - jb;
+    potf2_block_kernel<T, kDiagThreads><<<1, kDiagThreads, sizeof(T) * jb * jb, sp>>>(
+        at(j, j), rs, cs, jb, m > 0 ? winv : nullptr, nb, j, d_info, h->d_logdet);
+    ++h->launches;
+    CUCHOL_CHECK(cudaGetLastError());
+    if (m == 0) break;
+    T* P = pbuf[step & 1];
+
+    // panel solve: P = A21 * inv(L11)^H
+    GemmProblem<T> t = problem<T>();
+    t.a = at(j + jb, j); t.a_rs = rs; t.a_ks = cs;
+    t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1; t.tri_b = TRI_LOWER;
+    t.c = P; t.c_rs = 1; t.c_cs = ldp;
+    t.m = m; t.n = jb; t.k = jb;
+    CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
+    CUCHOL_CHECK_CU(copy_view<T>(h, P, 1, ldp, at(j + jb, j), rs, cs, m, jb, false, sp, d_info));
+    CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+
+    // lookahead: next block column, after the previous trailing update
+    const int jb2 = std::min(nb, m);
+    CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+    GemmProblem<T> u = problem<T>();
+    u.a = P; u.a_rs = 1; u.a_ks = ldp;
+    u.b = P; u.b_rs = 1; u.b_ks = ldp; u.conj_b = 1;
+    u.c = at(j + jb, j + jb); u.c_rs = rs; u.c_cs = cs;
+    u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
+    u.alpha = from_real<T>(RealOf<T>(-1)); u.beta = from_real<T>(RealOf<T>(1));
+    u.lower_only = 1; u.real_diag = 1;
+    u.m = m; u.n = jb2; u.k = jb;
+    CUCHOL_CHECK_CU(gemm<T>(h, u, sp, d_info));
+
+    // rest of the trailing matrix
+    if (m > jb2) {
+      CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+      GemmProblem<T> r = u;
+      r.a = P + jb2; r.b = P + jb2;
+      r.c = at(j + jb + jb2, j + jb + jb2); r.cin = r.c;
+      r.m = m - jb2; r.n = m - jb2;
+      CUCHOL_CHECK_CU(gemm<T>(h, r, su, d_info));
+      CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
+    }
+  }
+  CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
+  CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, d_info, sizeof(int), cudaMemcpyDeviceToHost, sp));
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_logdet, h->d_logdet, sizeof(double), cudaMemcpyDeviceToHost, sp));
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  *info = h->h_words[0];
+  if (logdet_out != nullptr) *logdet_out = h->h_logdet[0];
+  return CUDA_SUCCESS;
+}
+
+// ---- ?TRTRI ---------------------------------------------------------------------
+// Recursive in-place inverse of the logical lower triangle:
+//   [T11 0; T21 T22]^-1 = [T11^-1 0; -T22^-1 T21 T11^-1, T22^-1]
+// All nb x nb diagonal blocks are inverted in one launch, then the tree of splits
+// is walked bottom-up; every node of the same height is one grouped launch of
+//   X = T22^-1 T21       (TRMM, into workspace)
+//   T21 = -X T11^-1      (TRMM, back into A)
+// The first zero pivot is located before anything is modified: for lower storage
+// the reference's scan runs from the last column back (lapack/dtrtri.c:70-76), so
+// info is the largest zero position; for upper it is the smallest.
+struct Node { int o, s, s1, height; };
+
+int build_tree(int o, int s, int nb, std::vector<Node>& out) {
+  if (s <= nb) return 0;
+  int s1 = ((s / nb + 1) / 2) * nb;
+  int h1 = build_tree(o, s1, nb, out);
+  int h2 = build_tree(o + s1, s - s1, nb, out);
+  int hgt = 1 + std::max(h1, h2);
+  out.push_back({o, s, s1, hgt});
+  return hgt;
+}
+
+template <typename T>
+CUresult trtri_run(CULAPACKhandle h, bool upper, bool unit, int n, T* A, long long lda, long* info) {
+  const int nb = Tune<T>::nb;
+  const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
+  auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
+  cudaStream_t sp = h->s_panel;
+  *info = 0;
+  if (!unit) {
+    int init[3] = {0, 0, INT_MAX};
+    CUCHOL_CHECK(cudaMemcpyAsync(h->d_words, init, sizeof(init), cudaMemcpyHostToDevice, sp));
+    diag_scan_kernel<T><<<std::min((n + 255) / 256, 1024), 256, 0, sp>>>(A, rs + cs, n, h->d_words + 1);
+    ++h->launches;
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, h->d_words, 3 * sizeof(int), cudaMemcpyDeviceToHost, sp));
+    CUCHOL_CHECK(cudaStreamSynchronize(sp));
+    if (h->h_words[1] != 0) {
+      *info = upper ? h->h_words[2] : h->h_words[1];
+      return CUDA_SUCCESS;
+    }
+  }
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)trti2_batched_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
+  trti2_batched_kernel<T, kDiagThreads><<<(n + nb - 1) / nb, kDiagThreads, sizeof(T) * nb * nb, sp>>>(
+      A, rs, cs, n, nb, unit ? 1 : 0);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+
+  std::vector<Node> nodes;
+  const int height = build_tree(0, n, nb, nodes);
+  // workspace: X blocks of all nodes of one height side by side
+  size_t need = 0;
+  for (int hh = 1; hh <= height; ++hh) {
+    size_t lvl = 0;
+    for (auto& nd : nodes)
+      if (nd.height == hh) lvl += round_up((size_t)(nd.s - nd.s1), 2) * nd.s1;
+    need = std::max(need, lvl);
+  }
+  CUCHOL_CHECK_CU(ensure_workspace(h, sizeof(T) * std::max<size_t>(need, 1)));
+  h->desc_used = 0;
+  T* X = static_cast<T*>(h->ws);
+  for (int hh = 1; hh <= height; ++hh) {
+    std::vector<GemmProblem<T>> p1, p2;
+    size_t off = 0;
+    for (auto& nd : nodes) {
+      if (nd.height != hh) continue;
+      const int s1 = nd.s1, s2 = nd.s - nd.s1, o = nd.o;
+      const long long ldx = (long long)round_up((size_t)s2, 2);
+      T* x = X + off;
+      off += (size_t)ldx * s1;
+      GemmProblem<T> a = problem<T>();   // X = T22^-1 * T21
+      a.a = at(o + s1, o + s1); a.a_rs = rs; a.a_ks = cs; a.tri_a = TRI_LOWER; a.unit_a = unit;
+      a.b = at(o + s1, o); a.b_rs = cs; a.b_ks = rs;
+      a.c = x; a.c_rs = 1; a.c_cs = ldx;
+      a.m = s2; a.n = s1; a.k = s2;
+      p1.push_back(a);
+      GemmProblem<T> b = problem<T>();   // T21 = -X * T11^-1
+      b.a = x; b.a_rs = 1; b.a_ks = ldx;
+      b.b = at(o, o); b.b_rs = cs; b.b_ks = rs; b.tri_b = TRI_UPPER; b.unit_b = unit;
+      b.c = at(o + s1, o); b.c_rs = rs; b.c_cs = cs;
+      b.alpha = from_real<T>(RealOf<T>(-1));
+      b.m = s2; b.n = s1; b.k = s1;
+      p2.push_back(b);
+    }
+    CUCHOL_CHECK_CU(gemm_group<T>(h, p1, sp, nullptr));
+    CUCHOL_CHECK_CU(gemm_group<T>(h, p2, sp, nullptr));
+  }
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  return CUDA_SUCCESS;
+}
+
+// ---- ?LAUUM ---------------------------------------------------------------------
+// L^H L (lower; U U^H upper via the transposed view): every lower tile of the
+// result C(i, j) = sum_{k >= max(i,j)} conj(L(k, i)) L(k, j) is independent, so the
+// product is one launch into workspace, followed by a copy of its lower triangle
+// back into A.
+template <typename T>
+CUresult lauum_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda) {
+  const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
+  cudaStream_t sp = h->s_panel;
+  const long long ldw = (long long)round_up((size_t)n, 2);
+  CUCHOL_CHECK_CU(ensure_workspace(h, sizeof(T) * (size_t)ldw * n));
+  T* W = static_cast<T*>(h->ws);
+  GemmProblem<T> p = problem<T>();
+  p.a = A; p.a_rs = cs; p.a_ks = rs; p.conj_a = 1; p.tri_a = TRI_UPPER;
+  p.b = A; p.b_rs = cs; p.b_ks = rs; p.tri_b = TRI_UPPER;
+  p.c = W; p.c_rs = 1; p.c_cs = ldw;
+  p.m = n; p.n = n; p.k = n;
+  p.lower_only = 1; p.real_diag = 1;
+  CUCHOL_CHECK_CU(gemm<T>(h, p, sp, nullptr));
+  CUCHOL_CHECK_CU(copy_view<T>(h, W, 1, ldw, A, rs, cs, n, n, true, sp, nullptr));
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  return CUDA_SUCCESS;
+}
+
+// ---- ?TRTI22 (single block, caller stream, device info word) ---------------------
+template <typename T>
+CUresult trti22_run(CULAPACKhandle h, bool upper, bool unit, int n, const T* A, long long lda, T* B,
+                    long long ldb, int* dinfo, cudaStream_t stream) {
+  const long long ars = upper ? lda : 1, acs = upper ? 1 : lda;
+  const long long brs = upper ? ldb : 1, bcs = upper ? 1 : ldb;
+  const int nb = Tune<T>::nb;
+  if (n > nb) return CUDA_ERROR_INVALID_VALUE;
+  // info: zero pivots in the reference's scan order, then (if none) invert
+  int init[3] = {0, 0, INT_MAX};
+  CUCHOL_CHECK(cudaMemcpyAsync(h->d_words, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+  if (!unit) {
+    diag_scan_kernel<T><<<1, 128, 0, stream>>>(A, ars + acs, n, h->d_words + 1);
+    ++h->launches;
+    CUCHOL_CHECK(cudaGetLastError());
+  }
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, h->d_words, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CUCHOL_CHECK(cudaStreamSynchronize(stream));
+  int inf = (h->h_words[1] == 0) ? 0 : (upper ? h->h_words[2] : h->h_words[1]);
+  CUCHOL_CHECK(cudaMemcpyAsync(dinfo, &inf, sizeof(int), cudaMemcpyHostToDevice, stream));
+  CUCHOL_CHECK(cudaStreamSynchronize(stream));
+  if (inf != 0) return CUDA_SUCCESS;
+  if (A != B) CUCHOL_CHECK_CU(copy_view<T>(h, A, ars, acs, B, brs, bcs, n, n, true, stream, nullptr));
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)trti2_batched_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
+  trti2_batched_kernel<T, kDiagThreads><<<1, kDiagThreads, sizeof(T) * n * n, stream>>>(B, brs, bcs, n, n,
+                                                                                      unit ? 1 : 0);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+// ---- ?LOGDET --------------------------------------------------------------------
+template <typename T, typename Out>
+CUresult logdet_run(CULAPACKhandle h, const T* x, long long incx, long long n, Out* result, cudaStream_t stream) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, std::min(kLogdetMaxBlocks, 2 * h->num_sms));
+  logdet_kernel<T, 256><<<blocks, 256, 0, stream>>>(x, incx, n, h->d_part, h->d_counter, h->d_logdet + 1);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  if constexpr (sizeof(Out) == sizeof(double)) {
+    CUCHOL_CHECK(cudaMemcpyAsync(result, h->d_logdet + 1, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  } else {
+    // narrow on the device so the host copy stays asynchronous
+    narrow_double_kernel<<<1, 1, 0, stream>>>(h->d_logdet + 1, h->d_logdet_f);
+    ++h->launches;
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK(cudaMemcpyAsync(result, h->d_logdet_f, sizeof(float), cudaMemcpyDeviceToHost, stream));
+  }
+  return CUDA_SUCCESS;
+}
+
+}  // namespace
+
+
+// ------------------------------------------------------------------------------
+// Handle
+// ------------------------------------------------------------------------------
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
+  if (handle == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  auto* h = new (std::nothrow) __culapackhandle_st;
+  if (h == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
+  memset(h, 0, sizeof(*h));
+  CUCHOL_CHECK(cudaGetDevice(&h->device));
+  CUCHOL_CHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+  int lo = 0, hi = 0;
+  CUCHOL_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  // blocking streams: they order after work the caller queued on the legacy stream
+  CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_panel, cudaStreamDefault, hi));
+  CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_update, cudaStreamDefault, lo));
+  CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_panel, cudaEventDisableTiming));
+  CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_update, cudaEventDisableTiming));
+  CUCHOL_CHECK(cudaMalloc(&h->d_words, 16 * sizeof(int)));
+  CUCHOL_CHECK(cudaMallocHost(&h->h_words, 16 * sizeof(int)));
+  CUCHOL_CHECK(cudaMalloc(&h->d_logdet, 4 * sizeof(double)));
+  CUCHOL_CHECK(cudaMalloc(&h->d_logdet_f, 4 * sizeof(float)));
+  CUCHOL_CHECK(cudaMallocHost(&h->h_logdet, 4 * sizeof(double)));
+  CUCHOL_CHECK(cudaMalloc(&h->d_part, kLogdetMaxBlocks * sizeof(double)));
+  CUCHOL_CHECK(cudaMalloc(&h->d_counter, sizeof(unsigned int)));
+  CUCHOL_CHECK(cudaMemset(h->d_counter, 0, sizeof(unsigned int)));
+  h->desc_bytes = size_t(8) << 20;
+  CUCHOL_CHECK(cudaMalloc(&h->desc_dev, h->desc_bytes));
+  CUCHOL_CHECK(cudaMallocHost(&h->desc_host, h->desc_bytes));
+  CUCHOL_CHECK(cudaDeviceSynchronize());
+  *handle = h;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKDestroy(CULAPACKhandle h) {
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  CUCHOL_CHECK(cudaStreamSynchronize(h->s_panel));
+  CUCHOL_CHECK(cudaStreamSynchronize(h->s_update));
+  cudaFree(h->ws);
+  cudaFree(h->d_words);
+  cudaFreeHost(h->h_words);
+  cudaFree(h->d_logdet);
+  cudaFree(h->d_logdet_f);
+  cudaFreeHost(h->h_logdet);
+  cudaFree(h->d_part);
+  cudaFree(h->d_counter);
+  cudaFree(h->desc_dev);
+  cudaFreeHost(h->desc_host);
+  cudaEventDestroy(h->ev_panel);
+  cudaEventDestroy(h->ev_update);
+  cudaStreamDestroy(h->s_panel);
+  cudaStreamDestroy(h->s_update);
+  delete h;
+  return CUDA_SUCCESS;
+}
+
+// ------------------------------------------------------------------------------
+// C ABI.  Argument checks follow the reference drivers: lapack/dpotrf.c:173-179
+// (potrf, -4), lapack/dtrtri.c:330-336 (trtri, -5), lapack/dlauum.c (-4),
+// lapack/dpotri.c:29-35 (-4).  n == 0 returns at once.
+// ------------------------------------------------------------------------------
+namespace {
+
+inline bool bad_uplo(CBlasUplo u) { return u != CBlasLower && u != CBlasUpper; }
+
+template <typename T>
+CUresult api_potrf(const char* name, CULAPACKhandle h, CBlasUplo uplo, size_t n, CUdeviceptr A, size_t lda,
+                   long* info, double* logdet) {
+  *info = 0;
+  if (lda < n) *info = -4;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla(name, -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (n == 0) {
+    if (logdet) *logdet = 0.0;
+    return CUDA_SUCCESS;
+  }
+  if (h == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  return potrf_run<T>(h, uplo == CBlasUpper, (int)n, reinterpret_cast<T*>(A), (long long)lda, info, logdet);
+}
+
+template <typename T>
+CUresult api_trtri(const char* name, CULAPACKhandle h, CBlasUplo uplo, CBlasDiag diag, size_t n, CUdeviceptr A,
+                   size_t lda, long* info) {
+  *info = 0;
+  if (lda < n) *info = -5;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla(name, -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (n == 0) return CUDA_SUCCESS;
+  if (h == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  return trtri_run<T>(h, uplo == CBlasUpper, diag == CBlasUnit, (int)n, reinterpret_cast<T*>(A), (long long)lda,
+                      info);
+}
+
+template <typename T>
+CUresult api_lauum(const char* name, CULAPACKhandle h, CBlasUplo uplo, size_t n, CUdeviceptr A, size_t lda,
+                   long* info) {
+  *info = 0;
+  if (lda < n) *info = -4;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla(name, -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (n == 0) return CUDA_SUCCESS;
+  if (h == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  return lauum_run<T>(h, uplo == CBlasUpper, (int)n, reinterpret_cast<T*>(A), (long long)lda);
+}
+
+template <typename T>
+CUresult api_potri(const char* name, CULAPACKhandle h, CBlasUplo uplo, size_t n, CUdeviceptr A, size_t lda,
+                   long* info) {
+  *info = 0;
+  if (lda < n) *info = -4;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla(name, -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (n == 0) return CUDA_SUCCESS;
+  if (h == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  const bool up = (uplo == CBlasUpper);
+  CUCHOL_CHECK_CU(trtri_run<T>(h, up, false, (int)n, reinterpret_cast<T*>(A), (long long)lda, info));
+  if (*info != 0) return CUDA_SUCCESS;
+  return lauum_run<T>(h, up, (int)n, reinterpret_cast<T*>(A), (long long)lda);
+}
+
+template <typename T>
+CUresult api_trti22(CULAPACKhandle h, CBlasUplo uplo, CBlasDiag diag, size_t n, CUdeviceptr A, size_t lda,
+                    CUdeviceptr B, size_t ldb, CUdeviceptr info, CUstream stream) {
+  if (h == nullptr || bad_uplo(uplo) || lda < n || ldb < n) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0) return CUDA_SUCCESS;
+  return trti22_run<T>(h, uplo == CBlasUpper, diag == CBlasUnit, (int)n, reinterpret_cast<const T*>(A),
+                       (long long)lda, reinterpret_cast<T*>(B), (long long)ldb, reinterpret_cast<int*>(info),
+                       reinterpret_cast<cudaStream_t>(stream));
+}
+
+template <typename T, typename Out>
+CUresult api_logdet(CULAPACKhandle h, CUdeviceptr x, size_t incx, size_t n, Out* result, CUstream stream) {
+  if (n == 0) {
+    *result = Out(0);
+    return CUDA_SUCCESS;
+  }
+  if (h == nullptr || result == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  return logdet_run<T, Out>(h, reinterpret_cast<const T*>(x), (long long)incx, (long long)n, result,
+                            reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // namespace
+
+#define CUCHOL_API_TYPE(P, T, R)                                                                          \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##potrf(CULAPACKhandle h, CBlasUplo u, size_t n, CUdeviceptr A, size_t lda,    \
+                                   long* info) {                                                          \
+    return api_potrf<T>("cu" #P "potrf", h, u, n, A, lda, info, nullptr);                                 \
+  }                                                                                                       \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##trtri(CULAPACKhandle h, CBlasUplo u, CBlasDiag d, size_t n, CUdeviceptr A,   \
+                                   size_t lda, long* info) {                                              \
+    return api_trtri<T>("cu" #P "trtri", h, u, d, n, A, lda, info);                                       \
+  }                                                                                                       \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##lauum(CULAPACKhandle h, CBlasUplo u, size_t n, CUdeviceptr A, size_t lda,    \
+                                   long* info) {                                                          \
+    return api_lauum<T>("cu" #P "lauum", h, u, n, A, lda, info);                                          \
+  }                                                                                                       \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##potri(CULAPACKhandle h, CBlasUplo u, size_t n, CUdeviceptr A, size_t lda,    \
+                                   long* info) {                                                          \
+    return api_potri<T>("cu" #P "potri", h, u, n, A, lda, info);                                          \
+  }                                                                                                       \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##trti22(CULAPACKhandle h, CBlasUplo u, CBlasDiag d, size_t n, CUdeviceptr A,  \
+                                    size_t lda, CUdeviceptr B, size_t ldb, CUdeviceptr info, CUstream s) { \
+    return api_trti22<T>(h, u, d, n, A, lda, B, ldb, info, s);                                            \
+  }                                                                                                       \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##logdet(CULAPACKhandle h, CUdeviceptr x, size_t incx, size_t n, R* result,    \
+                                    CUstream s) {                                                         \
+    return api_logdet<T, R>(h, x, incx, n, result, s);                                                    \
+  }
+
+CUCHOL_API_TYPE(S, float, float)
+CUCHOL_API_TYPE(D, double, double)
+CUCHOL_API_TYPE(C, cuFloatComplex, float)
+CUCHOL_API_TYPE(Z, cuDoubleComplex, double)
+
+// ------------------------------------------------------------------------------
+// Extensions (include/cucholesky_ext.h)
+// ------------------------------------------------------------------------------
+#define CUCHOL_API_LOGDET(P, T)                                                                            \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##potrfLogdet(CULAPACKhandle h, CBlasUplo u, size_t n, CUdeviceptr A, \
+                                                       size_t lda, double* logdet, long* info) {           \
+    double ld = 0.0;                                                                                       \
+    CUresult r = api_potrf<T>("cu" #P "potrfLogdet", h, u, n, A, lda, info, &ld);                          \
+    if (r == CUDA_SUCCESS && *info == 0 && logdet != nullptr) *logdet = ld;                                \
+    return r;                                                                                              \
+  }
+CUCHOL_API_LOGDET(S, float)
+CUCHOL_API_LOGDET(D, double)
+CUCHOL_API_LOGDET(C, cuFloatComplex)
+CUCHOL_API_LOGDET(Z, cuDoubleComplex)
+
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKGetLaunchCount(CULAPACKhandle h, unsigned long long* count) {
+  if (h == nullptr || count == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  *count = h->launches;
+  return CUDA_SUCCESS;
+}

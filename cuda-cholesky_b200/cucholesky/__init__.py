@@ -1,0 +1,207 @@
+"""Python binding of libcucholesky.so, the sm_100a implementation of the dense SPD
+path (?POTRF, ?TRTRI, ?TRTI22, ?LAUUM, ?POTRI, ?LOGDET) behind the C API of
+``include/lapack.h``.
+
+The binding is a thin ctypes layer over that C ABI: every call goes through the
+exported ``cu?potrf`` / ``cu?potri`` / ... symbols with raw device pointers, the
+way a C caller of the reference library would call them.  Device memory comes
+from torch tensors (plumbing only).  There is no CPU fallback: if the shared
+library is missing, importing the binding's functions raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcucholesky.so")
+
+CUDA_SUCCESS = 0
+CUDA_ERROR_INVALID_VALUE = 1
+
+PREFIX = {"float32": "S", "float64": "D", "complex64": "C", "complex128": "Z"}
+
+_lib = None
+
+
+class CuCholeskyError(RuntimeError):
+    def __init__(self, name: str, code: int):
+        super().__init__(f"{name} returned CUresult {code}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Load libcucholesky.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C cuda-cholesky_b200/csrc` "
+                "(or __graft_entry__.build()); there is no fallback implementation")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L: C.CDLL) -> None:
+    H = C.c_void_p
+    for p in "SDCZ":
+        for name in ("potrf", "lauum", "potri"):
+            f = getattr(L, f"cu{p}{name}")
+            f.argtypes = [H, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.POINTER(C.c_long)]
+            f.restype = C.c_int
+        f = getattr(L, f"cu{p}trtri")
+        f.argtypes = [H, C.c_int, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.POINTER(C.c_long)]
+        f.restype = C.c_int
+        f = getattr(L, f"cu{p}trti22")
+        f.argtypes = [H, C.c_int, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t,
+                      C.c_uint64, C.c_void_p]
+        f.restype = C.c_int
+        f = getattr(L, f"cu{p}logdet")
+        out = C.c_float if p in "SC" else C.c_double
+        f.argtypes = [H, C.c_uint64, C.c_size_t, C.c_size_t, C.POINTER(out), C.c_void_p]
+        f.restype = C.c_int
+    L.cuLAPACKCreate.argtypes = [C.POINTER(C.c_void_p)]
+    L.cuLAPACKCreate.restype = C.c_int
+    L.cuLAPACKDestroy.argtypes = [C.c_void_p]
+    L.cuLAPACKDestroy.restype = C.c_int
+
+
+def exported_symbols() -> list[str]:
+    """Names a C caller links against (the include/lapack.h prototypes)."""
+    names = ["cuLAPACKCreate", "cuLAPACKDestroy", "xerbla", "errorHandler"]
+    for p in "SDCZ":
+        names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet")]
+    return names
+
+
+class Handle:
+    """CULAPACKhandle bound to the current CUDA device."""
+
+    def __init__(self):
+        self._h = C.c_void_p()
+        rc = lib().cuLAPACKCreate(C.byref(self._h))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuLAPACKCreate", rc)
+
+    @property
+    def value(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().cuLAPACKDestroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _uplo(u: str) -> int:
+    return ord(u.upper())
+
+
+def _prefix(t) -> str:
+    return PREFIX[str(t.dtype).replace("torch.", "")]
+
+
+def _lda(A) -> int:
+    """Column-major device matrix as a torch tensor of shape (n_cols, lda) in
+    row-major torch terms, i.e. A.T is the (lda, n) column-major matrix."""
+    return A.shape[1]
+
+
+# ---- raw C-ABI calls ------------------------------------------------------------
+
+def call_potrf(h: Handle, prefix: str, uplo: str, n: int, ptr: int, lda: int) -> tuple[int, int]:
+    info = C.c_long(0)
+    rc = getattr(lib(), f"cu{prefix}potrf")(h.value, _uplo(uplo), n, ptr, lda, C.byref(info))
+    return rc, info.value
+
+
+def call_potri(h: Handle, prefix: str, uplo: str, n: int, ptr: int, lda: int) -> tuple[int, int]:
+    info = C.c_long(0)
+    rc = getattr(lib(), f"cu{prefix}potri")(h.value, _uplo(uplo), n, ptr, lda, C.byref(info))
+    return rc, info.value
+
+
+def call_lauum(h: Handle, prefix: str, uplo: str, n: int, ptr: int, lda: int) -> tuple[int, int]:
+    info = C.c_long(0)
+    rc = getattr(lib(), f"cu{prefix}lauum")(h.value, _uplo(uplo), n, ptr, lda, C.byref(info))
+    return rc, info.value
+
+
+def call_trtri(h: Handle, prefix: str, uplo: str, diag: str, n: int, ptr: int, lda: int) -> tuple[int, int]:
+    info = C.c_long(0)
+    rc = getattr(lib(), f"cu{prefix}trtri")(h.value, _uplo(uplo), _uplo(diag), n, ptr, lda, C.byref(info))
+    return rc, info.value
+
+
+def call_trti22(h: Handle, prefix: str, uplo: str, diag: str, n: int, a: int, lda: int, b: int, ldb: int,
+                dinfo: int, stream: int = 0) -> int:
+    return getattr(lib(), f"cu{prefix}trti22")(h.value, _uplo(uplo), _uplo(diag), n, a, lda, b, ldb, dinfo,
+                                               C.c_void_p(stream))
+
+
+def call_logdet(h: Handle, prefix: str, ptr: int, incx: int, n: int, stream: int = 0) -> tuple[int, float]:
+    out = (C.c_float if prefix in "SC" else C.c_double)(0)
+    rc = getattr(lib(), f"cu{prefix}logdet")(h.value, ptr, incx, n, C.byref(out), C.c_void_p(stream))
+    return rc, out
+
+
+# ---- torch conveniences (column-major matrices as transposed torch tensors) ------
+
+def to_device_colmajor(A_np, device="cuda"):
+    """numpy (lda, n) Fortran-order array -> torch tensor T of shape (n, lda) whose
+    row j is column j of A, i.e. the same bytes as the column-major matrix."""
+    import numpy as np
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(A_np.T)).to(device)
+
+
+def to_host_colmajor(T):
+    import numpy as np
+    return np.asfortranarray(T.cpu().numpy().T)
+
+
+def potrf(h: Handle, T, n: int, uplo: str = "L") -> int:
+    rc, info = call_potrf(h, _prefix(T), uplo, n, T.data_ptr(), T.shape[1])
+    if rc != CUDA_SUCCESS:
+        raise CuCholeskyError(f"cu{_prefix(T)}potrf", rc)
+    return info
+
+
+def potri(h: Handle, T, n: int, uplo: str = "L") -> int:
+    rc, info = call_potri(h, _prefix(T), uplo, n, T.data_ptr(), T.shape[1])
+    if rc != CUDA_SUCCESS:
+        raise CuCholeskyError(f"cu{_prefix(T)}potri", rc)
+    return info
+
+
+def trtri(h: Handle, T, n: int, uplo: str = "L", diag: str = "N") -> int:
+    rc, info = call_trtri(h, _prefix(T), uplo, diag, n, T.data_ptr(), T.shape[1])
+    if rc != CUDA_SUCCESS:
+        raise CuCholeskyError(f"cu{_prefix(T)}trtri", rc)
+    return info
+
+
+def lauum(h: Handle, T, n: int, uplo: str = "L") -> int:
+    rc, info = call_lauum(h, _prefix(T), uplo, n, T.data_ptr(), T.shape[1])
+    if rc != CUDA_SUCCESS:
+        raise CuCholeskyError(f"cu{_prefix(T)}lauum", rc)
+    return info
+
+
+def logdet_of_factor(h: Handle, T, n: int) -> float:
+    """log det A from the factor in T (diagonal stride lda + 1), synchronising the
+    default stream before returning."""
+    import torch
+    lda = T.shape[1]
+    rc, out = call_logdet(h, _prefix(T), T.data_ptr(), lda + 1, n, 0)
+    if rc != CUDA_SUCCESS:
+        raise CuCholeskyError(f"cu{_prefix(T)}logdet", rc)
+    torch.cuda.synchronize()
+    return float(out.value)

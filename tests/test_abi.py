@@ -1,0 +1,88 @@
+"""The C ABI without a GPU: libcucholesky.so loads, exports every entry point that
+include/lapack.h declares, and the argument checks that run before any device
+work behave like the reference's (lapack/dpotrf.c:173-179)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+import cucholesky
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols() -> set[str]:
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:CUresult|void|int)\s+(cu\w+)\s*\(", text, flags=re.M))
+        names |= set(re.findall(r"^\s*extern\s+\w+\s+(\w+)\s*;", text, flags=re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = cucholesky.lib()
+    declared = _declared_symbols()
+    assert len(declared) >= 26
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", cucholesky.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert declared <= exported, sorted(declared - exported)
+    assert set(cucholesky.exported_symbols()) <= exported
+
+
+@pytest.mark.parametrize("p", list("SDCZ"))
+def test_argument_error_lda(p):
+    """lda < n: *info = -4 (-5 for trtri), XERBLA called with the position, and
+    CUDA_ERROR_INVALID_VALUE returned, before the handle is touched."""
+    lib = cucholesky.lib()
+    calls = []
+    XERBLA = C.CFUNCTYPE(None, C.c_char_p, C.c_long)
+
+    def hook(name, info):
+        calls.append((name.decode(), info))
+
+    cb = XERBLA(hook)
+    xer = C.c_void_p.in_dll(lib, "xerbla")
+    old = xer.value
+    xer.value = C.cast(cb, C.c_void_p).value
+    try:
+        for name, pos in (("potrf", 4), ("lauum", 4), ("potri", 4)):
+            info = C.c_long(0)
+            rc = getattr(lib, f"cu{p}{name}")(None, ord("L"), 10, 0, 5, C.byref(info))
+            assert rc == cucholesky.CUDA_ERROR_INVALID_VALUE
+            assert info.value == -pos
+            assert calls[-1] == (f"cu{p}{name}", pos)
+        info = C.c_long(0)
+        rc = getattr(lib, f"cu{p}trtri")(None, ord("U"), ord("N"), 10, 0, 5, C.byref(info))
+        assert rc == cucholesky.CUDA_ERROR_INVALID_VALUE and info.value == -5
+        assert calls[-1] == (f"cu{p}trtri", 5)
+    finally:
+        xer.value = old
+
+
+@pytest.mark.parametrize("p", list("SDCZ"))
+def test_empty_matrix_is_success(p):
+    lib = cucholesky.lib()
+    for name in ("potrf", "lauum", "potri"):
+        info = C.c_long(123)
+        assert getattr(lib, f"cu{p}{name}")(None, ord("L"), 0, 0, 0, C.byref(info)) == 0
+        assert info.value == 0
+    out = (C.c_float if p in "SC" else C.c_double)(5.0)
+    assert getattr(lib, f"cu{p}logdet")(None, 0, 1, 0, C.byref(out), None) == 0
+    assert out.value == 0.0
+
+
+def test_binding_fails_loudly_without_library(tmp_path, monkeypatch):
+    monkeypatch.setattr(cucholesky, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(cucholesky, "_lib", None)
+    with pytest.raises(FileNotFoundError):
+        cucholesky.lib()

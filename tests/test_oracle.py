@@ -1,0 +1,137 @@
+"""Pin the oracle: the plain-C restatement (oracle/oracle.c) against the golden
+vectors frozen from the reference library, and against the reference library
+itself (oracle/_ref) where it is built.  CPU only."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cucholesky import matgen
+
+TOL = {"s": 5e-5, "d": 1e-12, "c": 5e-5, "z": 1e-12}   # relative to max |A|
+
+
+def _keys(golden):
+    return sorted({k.rsplit("_", 1)[0] for k in golden.files if k.endswith("_info")})
+
+
+def _tri(u):
+    return np.tril if u == "L" else np.triu
+
+
+def test_golden_cases_present(golden):
+    keys = _keys(golden)
+    assert len(keys) >= 80
+    assert any("bad40" in k for k in keys)
+
+
+@pytest.mark.parametrize("p", list("sdcz"))
+def test_port_matches_golden(golden, p):
+    for key in _keys(golden):
+        if key[0] != p:
+            continue
+        u = key[1]
+        n, lda = (int(v) for v in key.split("_")[1:3])
+        A = golden[key + "_A"]
+        F = A.copy(order="F")
+        info = O.potrf(p, u, F, lda=lda, impl="port")
+        assert info == int(golden[key + "_info"]), key
+        Fg = golden[key + "_F"]
+        scale = np.abs(A[:n, :n]).max()
+        if info == 0:
+            d = np.abs(_tri(u)(F[:n, :n] - Fg[:n, :n])).max() / scale
+            assert d < TOL[p], (key, d)
+            X = F.copy(order="F")
+            assert O.potri(p, u, X, impl="port") == int(golden[key + "_Xinfo"])
+            Xg = golden[key + "_X"]
+            d = np.abs(_tri(u)(X[:n, :n] - Xg[:n, :n])).max() / max(np.abs(Xg[:n, :n]).max(), 1)
+            assert d < 50 * TOL[p], (key, d)
+            ld = O.logdet(p, F.ravel(order="F"), lda + 1, n, impl="port")
+            ref = float(golden[key + "_logdet"])
+            # the reference's c/z logdet sum logf(crealf(x)) (lapack/zlogdet.c:18)
+            tol = 1e-5 * max(1.0, abs(ref)) if p in "scz" else 1e-12 * max(1.0, abs(ref))
+            assert abs(ld - ref) <= tol, (key, ld, ref)
+        else:
+            # only the leading (info-1) x (info-1) part of a failed factor is defined
+            k = info - 1
+            d = np.abs(_tri(u)(F[:k, :k] - Fg[:k, :k])).max() / scale
+            assert d < TOL[p], (key, d)
+
+
+@pytest.mark.skipif(not O.available("reference"), reason="reference library not built")
+@pytest.mark.parametrize("p", list("sdcz"))
+@pytest.mark.parametrize("u", ["L", "U"])
+def test_port_matches_reference_library(p, u):
+    for n in (3, 40, 129, 200):
+        A = matgen.spd(p, n, seed=7 + n)
+        F1, F2 = A.copy(order="F"), A.copy(order="F")
+        assert O.potrf(p, u, F1, impl="port") == O.potrf(p, u, F2, impl="reference") == 0
+        d = np.abs(_tri(u)(F1 - F2)).max() / np.abs(A).max()
+        assert d < TOL[p], d
+        X1, X2 = F1.copy(order="F"), F2.copy(order="F")
+        assert O.potri(p, u, X1, impl="port") == O.potri(p, u, X2, impl="reference") == 0
+        d = np.abs(_tri(u)(X1 - X2)).max() / np.abs(X2).max()
+        assert d < 50 * TOL[p], d
+        for diag in "NU":
+            T1, T2 = F1.copy(order="F"), F1.copy(order="F")
+            assert O.trtri(p, u, T1, diag, impl="port") == O.trtri(p, u, T2, diag, impl="reference") == 0
+            d = np.abs(_tri(u)(T1 - T2)).max() / np.abs(T2).max()
+            assert d < 50 * TOL[p], d
+        L1, L2 = F1.copy(order="F"), F1.copy(order="F")
+        O.lauum(p, u, L1, impl="port")
+        O.lauum(p, u, L2, impl="reference")
+        d = np.abs(_tri(u)(L1 - L2)).max() / np.abs(L2).max()
+        assert d < 50 * TOL[p], d
+
+
+@pytest.mark.parametrize("p", list("sdcz"))
+@pytest.mark.parametrize("u", ["L", "U"])
+def test_port_error_bounds(p, u):
+    """Backward error and inverse residual of the oracle itself (bounds of the
+    parity contract: <= 10 in units of n*eps)."""
+    n = 96
+    A = matgen.spd(p, n, seed=3)
+    F = A.copy(order="F")
+    assert O.potrf(p, u, F) == 0
+    assert matgen.backward_error(A, F, u) <= 10
+    X = F.copy(order="F")
+    assert O.potri(p, u, X) == 0
+    assert matgen.inverse_residual(A, X, u) <= 10
+
+
+def test_info_config1_variant():
+    """The non-SPD variant of the FP64 n=2048 workload (A[1000][1000] = -1 after
+    construction) fails at leading minor 1001 in both CPU implementations."""
+    n = 2048
+    A = matgen.spd("d", n, seed=0)
+    A[1000, 1000] = -1.0
+    for impl in ("port", "reference"):
+        if not O.available(impl):
+            continue
+        for u in "LU":
+            F = A.copy(order="F")
+            assert O.potrf("d", u, F, impl=impl) == 1001
+
+
+def test_info_nan_and_zero_pivots():
+    n = 50
+    A = matgen.spd("d", n, seed=5)
+    A[17, 17] = np.nan
+    for u in "LU":
+        F = A.copy(order="F")
+        assert O.potrf("d", u, F) == 18
+    # trtri scan order: lower scans from the last column back, upper from the first
+    T = np.asfortranarray(np.tril(matgen.spd("d", 80, seed=6)))
+    T[10, 10] = 0.0
+    T[70, 70] = 0.0
+    assert O.trtri("d", "L", T.copy(order="F")) == 71
+    assert O.trtri("d", "U", np.asfortranarray(T.T.copy())) == 11
+    if O.available("reference"):
+        assert O.trtri("d", "L", T.copy(order="F"), impl="reference") == 71
+        assert O.trtri("d", "U", np.asfortranarray(T.T.copy()), impl="reference") == 11
+
+
+def test_argument_errors():
+    A = np.asfortranarray(np.eye(4))
+    assert O.potrf("d", "L", A, lda=3) == -4
