@@ -1,0 +1,416 @@
+// FP64 tensor-core tile engine for sm_100a (double precision).
+//
+// Blackwell's tcgen05.mma has no f64 kind, so FP64 products run on the warp-level
+// DMMA instruction mma.sync.aligned.m16n8k4.row.col.f64 (measured on B200: 37.1
+// TFLOP/s device-wide, the same rate as DFMA).  Operand tiles are staged into
+// shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle, no multicast)
+// through a 4-stage ring driven by mbarriers: one producer warp issues the copies,
+// four consumer warps (2 x 2, 64 x 32 each) run the MMAs on a 128 x 64 tile.
+//
+// Problem form: the GemmProblem of gemm.cuh for T = double,
+//     C(i, j) = alpha * sum_k Ahat(i, k) * Bhat(j, k) + beta * Cin(i, j),
+// with each view either row-contiguous (layout R: Ahat(i, k) = a[i + k*ld]) or
+// k-contiguous (layout K: Ahat(i, k) = a[i*ld + k]), 16-byte aligned with an even
+// leading dimension, optionally triangular (masked in registers on the k blocks
+// that cross the diagonal) and optionally lower-only in its output.
+//
+// Shared memory, one stage:
+//   layout R: BROWS/16 boxes of 16 rows x 16 k; a k-row is 128 bytes (16 doubles of
+//             consecutive rows), its 16-byte chunks XOR-swizzled by (k & 7);
+//   layout K: BROWS rows of 16 k (128 bytes), chunks swizzled by (row & 7).
+// The k order inside a 16-wide block is permuted: MMA step s (0..3), lane slot t
+// holds k = (s>>1)*8 + 2t + (s&1), so a K-layout thread reads the k pair of two
+// steps with one 128-bit load; an R-layout thread reads rows 2g, 2g+1 of one k with
+// one 128-bit load.  In both layouts the eight lanes of a quarter warp touch eight
+// distinct 16-byte chunks, so the fragment loads are bank-conflict free.
+#pragma once
+#include <cuda.h>
+#include <stdint.h>
+#include "gemm.cuh"
+
+namespace cuchol {
+namespace dmma {
+
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 4;
+constexpr int CONSUMERS = 4;                       // 2 x 2 warps of 64 x 32
+constexpr int THREADS = (CONSUMERS + 1) * 32;
+constexpr int A_STAGE = BM * BK * 8;               // 16 KB
+constexpr int B_STAGE = BN * BK * 8;               // 8 KB
+constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
+constexpr unsigned kSpinLimit = 1u << 26;          // bounded mbarrier waits (~seconds)
+
+enum : int { LAYOUT_R = 0, LAYOUT_K = 1 };
+
+struct Params {
+  double* c; long long c_rs, c_cs;
+  const double* cin; long long cin_rs, cin_cs;
+  int m, n, k;
+  double alpha, beta;
+  int tri_a, tri_b, unit_a, unit_b;
+  int lower_only;
+  int tiles_n;
+  int vec_ok;            // C / Cin 16-byte aligned along their unit stride, Cin == C
+  int preload;           // alpha = +-1: accumulators start at beta*Cin (loaded before
+                         // the k loop, so its latency hides under the TMA fill)
+  int neg;               // alpha = -1 (with preload): B fragments are negated
+  int* err;              // set when a bounded wait gave up
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (unsigned it = 0; it < kSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+__device__ __forceinline__ int fperm(int g) { return (g >> 1) | ((g & 1) << 2); }
+
+// Issue the TMA copies of one operand tile (rows [r0, r0 + ROWS), k [k0, k0 + 16)).
+template <int L, int ROWS>
+__device__ __forceinline__ void load_operand(const CUtensorMap* map, uint64_t* bar, unsigned char* dst, int r0, int k0) {
+  if constexpr (L == LAYOUT_R) {
+#pragma unroll
+    for (int b = 0; b < ROWS / 16; ++b) tma_load_2d(map, bar, dst + b * 2048, r0 + 16 * b, k0);
+  } else {
+    tma_load_2d(map, bar, dst, k0, r0);
+  }
+}
+
+// Mask one loaded fragment value of a triangular view: (row, k) outside the
+// triangle reads zero, a unit diagonal reads one.
+__device__ __forceinline__ double tri_mask(double v, int tri, int unit, int row, int k) {
+  if (unit && row == k) return 1.0;
+  if (tri == TRI_LOWER && k > row) return 0.0;
+  if (tri == TRI_UPPER && k < row) return 0.0;
+  return v;
+}
+
+template <int LA, int LB, bool TRI>
+__global__ void __maxnreg__(200)
+gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+            const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
+  if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
+  const int tile = blockIdx.x;
+  const int ti = tile / P.tiles_n, tj = tile % P.tiles_n;
+  const int i0 = ti * BM, j0 = tj * BN;
+  if (P.lower_only && j0 > i0 + BM - 1) return;
+
+  // k range of this tile (triangular views limit it), aligned down to BK
+  int kb = 0, ke = P.k;
+  if (P.tri_a == TRI_LOWER) ke = min(ke, i0 + BM);
+  if (P.tri_a == TRI_UPPER) kb = max(kb, i0);
+  if (P.tri_b == TRI_LOWER) ke = min(ke, j0 + BN);
+  if (P.tri_b == TRI_UPPER) kb = max(kb, j0);
+  const int kbase = (kb / BK) * BK;
+  const int KT = (ke > kbase) ? (ke - kbase + BK - 1) / BK : 0;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES];
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], CONSUMERS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == CONSUMERS) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      int issued = 0;
+      bool ok = true;
+      for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt % STAGES;
+        if (kt >= STAGES && !mbar_wait(&empty_bar[s], ((kt / STAGES) - 1) & 1)) { ok = false; break; }
+        unsigned char* st = smem + s * STAGE_BYTES;
+        mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+        load_operand<LA, BM>(&mapA, &full_bar[s], st, i0, kbase + kt * BK);
+        load_operand<LB, BN>(&mapB, &full_bar[s], st + A_STAGE, j0, kbase + kt * BK);
+        issued = kt + 1;
+      }
+      if (!ok) atomicExch(P.err, 1);
+      // every issued copy must have landed before the CTA may exit
+      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
+        if (!mbar_wait(&full_bar[kt % STAGES], (kt / STAGES) & 1)) atomicExch(P.err, 2);
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const int wm = warp & 1, wn = warp >> 1;
+  const int g = lane >> 2, t = lane & 3;
+  const int fg = fperm(g);
+  // rows of this thread's A fragments inside an m16 block (a0, a1) and the column
+  // of its B fragment inside an n8 block, per layout
+  const int arow0 = (LA == LAYOUT_R) ? 2 * g : fg;
+  const int arow1 = (LA == LAYOUT_R) ? 2 * g + 1 : fg + 8;
+  double acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+
+  const int wrow = i0 + wm * 64, wcol = j0 + wn * 32;   // first row / column of the warp
+  // acc[mb][nb8][e]: row = wrow + mb*16 + (e < 2 ? arow0 : arow1),
+  //                  col = wcol + colof(nb8, e & 1)
+  auto colof = [&](int nb8, int e1) -> int {
+    if constexpr (LB == LAYOUT_R) return (nb8 >> 1) * 16 + 4 * t + 2 * e1 + (nb8 & 1);
+    else return nb8 * 8 + t + 4 * e1;
+  };
+  const bool full_tile = (i0 + BM <= P.m) && (j0 + BN <= P.n) && (!P.lower_only || j0 + BN - 1 <= i0);
+  const bool vec_rows = (LA == LAYOUT_R) && full_tile && P.vec_ok && P.c_rs == 1;
+  const bool vec_cols = !vec_rows && (LB == LAYOUT_R) && full_tile && P.vec_ok && P.c_cs == 1;
+  if (P.preload && P.cin != nullptr) {
+    if (vec_rows) {
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+        for (int nb8 = 0; nb8 < 4; ++nb8)
+#pragma unroll
+          for (int e1 = 0; e1 < 2; ++e1) {
+            const int row = wrow + mb * 16 + arow0, col = wcol + colof(nb8, e1);
+            const double2 o = *reinterpret_cast<const double2*>(P.cin + row + (long long)col * P.cin_cs);
+            acc[mb][nb8][e1] = P.beta * o.x;
+            acc[mb][nb8][2 + e1] = P.beta * o.y;
+          }
+    } else if (vec_cols) {
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+          for (int p = 0; p < 2; ++p) {
+            const int row = wrow + mb * 16 + (e < 2 ? arow0 : arow1);
+            const int col = wcol + colof(2 * p, e & 1);
+            const double2 o = *reinterpret_cast<const double2*>(P.cin + (long long)row * P.cin_rs + col);
+            acc[mb][2 * p][e] = P.beta * o.x;
+            acc[mb][2 * p + 1][e] = P.beta * o.y;
+          }
+    } else {
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+        for (int nb8 = 0; nb8 < 4; ++nb8)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int row = wrow + mb * 16 + (e < 2 ? arow0 : arow1);
+            const int col = wcol + colof(nb8, e & 1);
+            if (row < P.m && col < P.n && (!P.lower_only || row >= col))
+              acc[mb][nb8][e] = P.beta * P.cin[row * P.cin_rs + (long long)col * P.cin_cs];
+          }
+    }
+  }
+  bool ok = true;
+  for (int kt = 0; kt < KT; ++kt) {
+    const int s = kt % STAGES;
+    if (!mbar_wait(&full_bar[s], (kt / STAGES) & 1)) { ok = false; break; }
+    const unsigned char* As = smem + s * STAGE_BYTES;
+    const unsigned char* Bs = As + A_STAGE;
+    const int ks = kbase + kt * BK;
+    const bool mask_a = TRI && ((P.tri_a == TRI_LOWER && ks + BK - 1 >= wrow) ||
+                                (P.tri_a == TRI_UPPER && ks <= wrow + 63));
+    const bool mask_b = TRI && ((P.tri_b == TRI_LOWER && ks + BK - 1 >= wcol) ||
+                                (P.tri_b == TRI_UPPER && ks <= wcol + 31));
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {            // pairs of MMA k-steps (2q, 2q + 1)
+      // B fragments for both steps of the pair
+      double2 bv[4];
+      if constexpr (LB == LAYOUT_R) {
+        // bv[2p + s2] = (column 2g of box p, column 2g + 1) at the k of step 2q + s2
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          const unsigned char* box = Bs + (wn * 2 + p) * 2048;
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const int k = q * 8 + 2 * t + s2;
+            bv[2 * p + s2] = *reinterpret_cast<const double2*>(box + k * 128 + ((g ^ (k & 7)) << 4));
+          }
+        }
+      } else {
+        // bv[nb8] = (k of step 2q, k of step 2q + 1) at column fg of n8 block nb8
+        const int ch = q * 4 + t;
+#pragma unroll
+        for (int nb8 = 0; nb8 < 4; ++nb8) {
+          const int r = wn * 32 + nb8 * 8 + fg;
+          bv[nb8] = *reinterpret_cast<const double2*>(Bs + r * 128 + ((ch ^ (r & 7)) << 4));
+        }
+      }
+      if (mask_b) {
+        if constexpr (LB == LAYOUT_R) {
+#pragma unroll
+          for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+              const int k = ks + q * 8 + 2 * t + s2;
+              const int cb = wcol + p * 16 + 2 * g;
+              bv[2 * p + s2].x = tri_mask(bv[2 * p + s2].x, P.tri_b, P.unit_b, cb, k);
+              bv[2 * p + s2].y = tri_mask(bv[2 * p + s2].y, P.tri_b, P.unit_b, cb + 1, k);
+            }
+        } else {
+#pragma unroll
+          for (int nb8 = 0; nb8 < 4; ++nb8) {
+            const int k = ks + q * 8 + 2 * t;
+            const int cb = wcol + nb8 * 8 + fg;
+            bv[nb8].x = tri_mask(bv[nb8].x, P.tri_b, P.unit_b, cb, k);
+            bv[nb8].y = tri_mask(bv[nb8].y, P.tri_b, P.unit_b, cb, k + 1);
+          }
+        }
+      }
+      if (P.neg) {   // after the triangle mask, so an implicit unit diagonal is negated too
+#pragma unroll
+        for (int v = 0; v < 4; ++v) bv[v] = make_double2(-bv[v].x, -bv[v].y);
+      }
+#pragma unroll
+      for (int mb = 0; mb < 4; ++mb) {
+        // A fragments of m16 block mb: av[s2] = (row arow0, row arow1) at step 2q + s2
+        double2 av[2];
+        if constexpr (LA == LAYOUT_R) {
+          const unsigned char* box = As + (wm * 4 + mb) * 2048;
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const int k = q * 8 + 2 * t + s2;
+            av[s2] = *reinterpret_cast<const double2*>(box + k * 128 + ((g ^ (k & 7)) << 4));
+          }
+        } else {
+          const int r0 = wm * 64 + mb * 16 + fg, r1 = r0 + 8;
+          const int ch = q * 4 + t;
+          const double2 x0 = *reinterpret_cast<const double2*>(As + r0 * 128 + ((ch ^ (r0 & 7)) << 4));
+          const double2 x1 = *reinterpret_cast<const double2*>(As + r1 * 128 + ((ch ^ (r1 & 7)) << 4));
+          av[0] = make_double2(x0.x, x1.x);
+          av[1] = make_double2(x0.y, x1.y);
+        }
+        if (mask_a) {
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const int k = ks + q * 8 + 2 * t + s2;
+            const int ra = wrow + mb * 16;
+            av[s2].x = tri_mask(av[s2].x, P.tri_a, P.unit_a, ra + arow0, k);
+            av[s2].y = tri_mask(av[s2].y, P.tri_a, P.unit_a, ra + arow1, k);
+          }
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+          for (int nb8 = 0; nb8 < 4; ++nb8) {
+            double b;
+            if constexpr (LB == LAYOUT_R) {
+              const double2 v = bv[2 * (nb8 >> 1) + s2];
+              b = (nb8 & 1) ? v.y : v.x;
+            } else {
+              b = s2 ? bv[nb8].y : bv[nb8].x;
+            }
+            dmma_16x8x4(acc[mb][nb8], av[s2].x, av[s2].y, b);
+          }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty_bar[s]);
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(P.err, 3);
+    return;
+  }
+
+  // ---------------- epilogue ----------------
+  // preload: C = acc; otherwise C = alpha * acc + beta * Cin
+  const bool has_cin = (P.cin != nullptr) && !P.preload;
+  const double alpha = P.preload ? 1.0 : P.alpha;
+  if (vec_rows) {
+    // column-major C: rows arow0 and arow0 + 1 are adjacent
+#pragma unroll
+    for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+      for (int nb8 = 0; nb8 < 4; ++nb8)
+#pragma unroll
+        for (int e1 = 0; e1 < 2; ++e1) {
+          const int row = wrow + mb * 16 + arow0, col = wcol + colof(nb8, e1);
+          double2* ptr = reinterpret_cast<double2*>(P.c + row + (long long)col * P.c_cs);
+          double2 v = make_double2(alpha * acc[mb][nb8][e1], alpha * acc[mb][nb8][2 + e1]);
+          if (has_cin) {
+            const double2 o = *ptr;
+            v.x = fma(P.beta, o.x, v.x);
+            v.y = fma(P.beta, o.y, v.y);
+          }
+          *ptr = v;
+        }
+  } else if (vec_cols) {
+    // row-contiguous C: the columns of n8 blocks 2p and 2p + 1 are adjacent
+#pragma unroll
+    for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          const int row = wrow + mb * 16 + (e < 2 ? arow0 : arow1);
+          const int col = wcol + colof(2 * p, e & 1);
+          double2* ptr = reinterpret_cast<double2*>(P.c + (long long)row * P.c_rs + col);
+          double2 v = make_double2(alpha * acc[mb][2 * p][e], alpha * acc[mb][2 * p + 1][e]);
+          if (has_cin) {
+            const double2 o = *ptr;
+            v.x = fma(P.beta, o.x, v.x);
+            v.y = fma(P.beta, o.y, v.y);
+          }
+          *ptr = v;
+        }
+  } else {
+#pragma unroll
+    for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+      for (int nb8 = 0; nb8 < 4; ++nb8)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int row = wrow + mb * 16 + (e < 2 ? arow0 : arow1);
+          const int col = wcol + colof(nb8, e & 1);
+          if (row < P.m && col < P.n && (!P.lower_only || row >= col)) {
+            double v = alpha * acc[mb][nb8][e];
+            if (has_cin) v = fma(P.beta, P.cin[row * P.cin_rs + (long long)col * P.cin_cs], v);
+            P.c[row * P.c_rs + (long long)col * P.c_cs] = v;
+          }
+        }
+  }
+}
+
+}  // namespace dmma
+}  // namespace cuchol

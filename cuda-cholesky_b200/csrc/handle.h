@@ -12,7 +12,8 @@ struct __culapackhandle_st {
   cudaStream_t s_panel;    // diagonal block, panel solve, lookahead update (high priority)
   cudaStream_t s_update;   // trailing update
   cudaEvent_t ev_panel, ev_update;
-  int* d_words;            // device scratch words: [0] info, [1] scan max, [2] scan min
+  int* d_words;            // device scratch words: [0] info, [1] scan max, [2] scan min,
+                           // [3] engine error (a bounded wait gave up)
   int* h_words;            // pinned mirror of d_words
   double* d_logdet;        // [0] fused potrf log det, [1] ?logdet result (double)
   float* d_logdet_f;       // ?logdet result (float)
@@ -26,6 +27,7 @@ struct __culapackhandle_st {
   size_t desc_bytes, desc_used;
   int num_sms;
   unsigned long long launches;   // kernels launched by this handle
+  int force_simt;                // testing: route FP64 products to the SIMT engine
 };
 
 namespace cuchol {

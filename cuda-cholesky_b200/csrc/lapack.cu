@@ -7,12 +7,16 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "diag.cuh"
+#include "dmma.cuh"
 #include "gemm.cuh"
 #include "handle.h"
+#include "panel.cuh"
 
 using namespace cuchol;
 
@@ -99,9 +103,112 @@ CUresult launch_dispatch(CULAPACKhandle h, const GemmLaunch<T>& L, int tiles, in
 
 constexpr int kTile = 64;
 
+// ---- FP64 tensor-core path (dmma.cuh) --------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// FP64 view (rows x k) as a TMA map with 128-byte swizzle; rows / k beyond the
+// view read as zero.  Layout R (rows contiguous): 16 x 16 boxes.  Layout K (k
+// contiguous): boxes of 16 k x box_rows rows.
+bool make_map(CUtensorMap* map, const double* base, int layout, long long rows, long long k, long long ld,
+              int box_rows) {
+  EncodeTiledFn fn = encode_tiled();
+  if (fn == nullptr) return false;
+  cuuint64_t dims[2], strides[1] = {(cuuint64_t)ld * sizeof(double)};
+  cuuint32_t box[2], estr[2] = {1, 1};
+  if (layout == dmma::LAYOUT_R) {
+    dims[0] = rows; dims[1] = k; box[0] = 16; box[1] = 16;
+  } else {
+    dims[0] = k; dims[1] = rows; box[0] = 16; box[1] = box_rows;
+  }
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+template <int LA, int LB, bool TRI>
+CUresult launch_dmma(CULAPACKhandle h, const CUtensorMap& ma, const CUtensorMap& mb, const dmma::Params& q,
+                     int tiles, cudaStream_t s, const int* abort) {
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      dmma::SMEM_BYTES));
+    attr = true;
+  }
+  dmma::gemm_kernel<LA, LB, TRI><<<tiles, dmma::THREADS, dmma::SMEM_BYTES, s>>>(ma, mb, q, abort);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+template <bool TRI>
+CUresult launch_dmma_layouts(CULAPACKhandle h, int la, int lb, const CUtensorMap& ma, const CUtensorMap& mb,
+                             const dmma::Params& q, int tiles, cudaStream_t s, const int* abort) {
+  if (la == 0 && lb == 0) return launch_dmma<0, 0, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 1) return launch_dmma<0, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 1 && lb == 0) return launch_dmma<1, 0, TRI>(h, ma, mb, q, tiles, s, abort);
+  return launch_dmma<1, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+}
+
+// Runs the problem on the FP64 tensor-core engine if its views fit the engine
+// (each view row- or k-contiguous, 16-byte aligned, even leading dimension);
+// returns false (nothing launched) otherwise.
+bool try_dmma(CULAPACKhandle h, const GemmProblem<double>& p, cudaStream_t s, const int* abort, CUresult* rc) {
+  const int la = (p.a_rs == 1) ? dmma::LAYOUT_R : (p.a_ks == 1 ? dmma::LAYOUT_K : -1);
+  const int lb = (p.b_rs == 1) ? dmma::LAYOUT_R : (p.b_ks == 1 ? dmma::LAYOUT_K : -1);
+  if (la < 0 || lb < 0 || p.k <= 0) return false;
+  const long long lda = (la == dmma::LAYOUT_R) ? p.a_ks : p.a_rs;
+  const long long ldb = (lb == dmma::LAYOUT_R) ? p.b_ks : p.b_rs;
+  if ((lda & 1) || (ldb & 1) || !aligned16(p.a) || !aligned16(p.b)) return false;
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, p.a, la, p.m, p.k, lda, dmma::BM) || !make_map(&mb, p.b, lb, p.n, p.k, ldb, dmma::BN))
+    return false;
+  dmma::Params q;
+  q.c = p.c; q.c_rs = p.c_rs; q.c_cs = p.c_cs;
+  q.cin = p.cin; q.cin_rs = p.cin_rs; q.cin_cs = p.cin_cs;
+  q.m = p.m; q.n = p.n; q.k = p.k;
+  q.alpha = p.alpha; q.beta = p.beta;
+  q.tri_a = p.tri_a; q.tri_b = p.tri_b; q.unit_a = p.unit_a; q.unit_b = p.unit_b;
+  q.lower_only = p.lower_only;
+  q.tiles_n = (p.n + dmma::BN - 1) / dmma::BN;
+  const long long other = (p.c_rs == 1) ? p.c_cs : p.c_rs;
+  q.vec_ok = aligned16(p.c) && !(other & 1) &&
+             (p.cin == nullptr || (p.cin == p.c && p.cin_rs == p.c_rs && p.cin_cs == p.c_cs));
+  q.preload = (p.alpha == 1.0 || p.alpha == -1.0) &&
+              (p.cin == nullptr || (p.cin_rs == p.c_rs && p.cin_cs == p.c_cs) || p.cin != p.c);
+  q.neg = q.preload && p.alpha == -1.0;
+  q.err = h->d_words + 3;
+  const int tiles = ((p.m + dmma::BM - 1) / dmma::BM) * q.tiles_n;
+  const bool tri = p.tri_a || p.tri_b || p.unit_a || p.unit_b;
+  *rc = tri ? launch_dmma_layouts<true>(h, la, lb, ma, mb, q, tiles, s, abort)
+            : launch_dmma_layouts<false>(h, la, lb, ma, mb, q, tiles, s, abort);
+  return true;
+}
+
 template <typename T>
 CUresult gemm(CULAPACKhandle h, GemmProblem<T> p, cudaStream_t s, const int* abort) {
   if (p.m <= 0 || p.n <= 0) return CUDA_SUCCESS;
+  if constexpr (std::is_same<T, double>::value) {
+    CUresult rc;
+    if (!h->force_simt && try_dmma(h, p, s, abort, &rc)) return rc;
+  }
   p.tiles_n = (p.n + kTile - 1) / kTile;
   p.tile_begin = 0;
   const int tiles = ((p.m + kTile - 1) / kTile) * p.tiles_n;
@@ -122,7 +229,11 @@ CUresult gemm_group(CULAPACKhandle h, std::vector<GemmProblem<T>>& ps, cudaStrea
     p.tile_begin = tiles;
     tiles += ((p.m + kTile - 1) / kTile) * p.tiles_n;
   }
-  if (ps.size() == 1) return gemm<T>(h, ps[0], s, abort);
+  // few problems: one launch each, so FP64 ones reach the tensor-core engine
+  if (ps.size() <= 8) {
+    for (auto& p : ps) CUCHOL_CHECK_CU(gemm<T>(h, p, s, abort));
+    return CUDA_SUCCESS;
+  }
   void* dev = stage_descriptors(h, ps.data(), ps.size() * sizeof(GemmProblem<T>), s);
   if (dev == nullptr) {   // list area full: one launch per problem
     for (auto& p : ps) CUCHOL_CHECK_CU(gemm<T>(h, p, s, abort));
@@ -154,6 +265,17 @@ CUresult copy_view(CULAPACKhandle h, const T* src, long long s_rs, long long s_c
   return CUDA_SUCCESS;
 }
 
+// A bounded wait inside an engine kernel gave up (h_words mirrors d_words):
+// report it as a launch timeout and clear the word for the next call.
+CUresult check_engine(CULAPACKhandle h) {
+  if (h->h_words[3] == 0) return CUDA_SUCCESS;
+  h->h_words[3] = 0;
+  CUCHOL_CHECK(cudaMemset(h->d_words + 3, 0, sizeof(int)));
+  if (errorHandler != nullptr)
+    errorHandler("engine wait", __func__, __FILE__, __LINE__, (int)CUDA_ERROR_LAUNCH_TIMEOUT, &error_string);
+  return CUDA_ERROR_LAUNCH_TIMEOUT;
+}
+
 template <typename T>
 CUresult set_smem(const void* fn, size_t bytes) {
   CUCHOL_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -162,17 +284,22 @@ CUresult set_smem(const void* fn, size_t bytes) {
 
 // ---- ?POTRF ---------------------------------------------------------------------
 // Right-looking blocked Cholesky with lookahead depth 1, on two streams:
-//   panel stream : diagonal block (factor + inverse)  -> panel solve into P
-//                  -> copy P into A -> [wait trailing update of the previous step]
-//                  -> update of the next block column (lookahead)
-//   update stream: [wait panel] -> update of the rest of the trailing matrix
-// so the next diagonal block and panel are factored while the previous trailing
-// update is still running.  P is a ping-pong pair of packed panel buffers.
-// Failure: the diagonal-block kernel sets the device info word, and every later
-// kernel exits at entry when it is set.
+//   panel stream : diagonal-block factor + inverse W (one CTA) -> panel solve
+//                  P = A21 W^H (tensor-core GEMM into the packed buffer P)
+//                  -> [wait previous trailing update] -> update of the next block
+//                  column (lookahead)
+//   update stream: [wait panel] -> copy P into A21 -> update of the rest of the
+//                  trailing matrix
+// so the next panel is factored on a few SMs while the previous trailing update
+// still runs on the rest.  P is a ping-pong pair of packed panel buffers.
+// Failure: the diagonal kernel sets the device info word, and every later kernel
+// exits at entry when it is set.
+constexpr int kDiagThreads2 = 256;
+
 template <typename T>
 CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out) {
-  const int nb = Tune<T>::nb;
+  constexpr int nb = Tune<T>::nb;
+  using Smem = DiagSmem<T, nb>;
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
   auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
   cudaStream_t sp = h->s_panel, su = h->s_update;
@@ -184,32 +311,36 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   T* winv = static_cast<T*>(h->ws);
   T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * nb};
 
-  CUCHOL_CHECK_CU(set_smem<T>((const void*)potf2_block_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_factor_kernel<T, nb, kDiagThreads2>, Smem::bytes));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
   CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
   // the update stream starts after the panel stream's initialisation
   CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
   CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+  CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
 
   for (int j = 0, step = 0; j < n; j += nb, ++step) {
     const int jb = std::min(nb, n - j);
     const int m = n - j - jb;
-    potf2_block_kernel<T, kDiagThreads><<<1, kDiagThreads, sizeof(T) * jb * jb, sp>>>(
+    diag_factor_kernel<T, nb, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
         at(j, j), rs, cs, jb, m > 0 ? winv : nullptr, nb, j, d_info, h->d_logdet);
     ++h->launches;
     CUCHOL_CHECK(cudaGetLastError());
     if (m == 0) break;
     T* P = pbuf[step & 1];
 
-    // panel solve: P = A21 * inv(L11)^H
+    // panel solve: P = A21 * inv(L11)^H (W holds explicit zeros above its diagonal)
     GemmProblem<T> t = problem<T>();
     t.a = at(j + jb, j); t.a_rs = rs; t.a_ks = cs;
-    t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1; t.tri_b = TRI_LOWER;
+    t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;
     t.c = P; t.c_rs = 1; t.c_cs = ldp;
     t.m = m; t.n = jb; t.k = jb;
     CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
-    CUCHOL_CHECK_CU(copy_view<T>(h, P, 1, ldp, at(j + jb, j), rs, cs, m, jb, false, sp, d_info));
     CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+
+    // update stream: the solved panel into A, off the panel stream's critical path
+    CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+    CUCHOL_CHECK_CU(copy_view<T>(h, P, 1, ldp, at(j + jb, j), rs, cs, m, jb, false, su, d_info));
 
     // lookahead: next block column, after the previous trailing update
     const int jb2 = std::min(nb, m);
@@ -226,20 +357,21 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
 
     // rest of the trailing matrix
     if (m > jb2) {
-      CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
       GemmProblem<T> r = u;
       r.a = P + jb2; r.b = P + jb2;
       r.c = at(j + jb + jb2, j + jb + jb2); r.cin = r.c;
       r.m = m - jb2; r.n = m - jb2;
       CUCHOL_CHECK_CU(gemm<T>(h, r, su, d_info));
-      CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
     }
+    // always recorded: it also covers the copy that still reads P
+    CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   }
   CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
-  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, d_info, sizeof(int), cudaMemcpyDeviceToHost, sp));
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, d_info, 4 * sizeof(int), cudaMemcpyDeviceToHost, sp));
   CUCHOL_CHECK(cudaMemcpyAsync(h->h_logdet, h->d_logdet, sizeof(double), cudaMemcpyDeviceToHost, sp));
   CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  CUCHOL_CHECK_CU(check_engine(h));
   *info = h->h_words[0];
   if (logdet_out != nullptr) *logdet_out = h->h_logdet[0];
   return CUDA_SUCCESS;
@@ -287,8 +419,9 @@ CUresult trtri_run(CULAPACKhandle h, bool upper, bool unit, int n, T* A, long lo
       return CUDA_SUCCESS;
     }
   }
-  CUCHOL_CHECK_CU(set_smem<T>((const void*)trti2_batched_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
-  trti2_batched_kernel<T, kDiagThreads><<<(n + nb - 1) / nb, kDiagThreads, sizeof(T) * nb * nb, sp>>>(
+  constexpr int NB = Tune<T>::nb;
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_invert_kernel<T, NB, kDiagThreads2>, DiagSmem<T, NB>::bytes));
+  diag_invert_kernel<T, NB, kDiagThreads2><<<(n + nb - 1) / nb, kDiagThreads2, DiagSmem<T, NB>::bytes, sp>>>(
       A, rs, cs, n, nb, unit ? 1 : 0);
   ++h->launches;
   CUCHOL_CHECK(cudaGetLastError());
@@ -383,9 +516,10 @@ CUresult trti22_run(CULAPACKhandle h, bool upper, bool unit, int n, const T* A, 
   CUCHOL_CHECK(cudaStreamSynchronize(stream));
   if (inf != 0) return CUDA_SUCCESS;
   if (A != B) CUCHOL_CHECK_CU(copy_view<T>(h, A, ars, acs, B, brs, bcs, n, n, true, stream, nullptr));
-  CUCHOL_CHECK_CU(set_smem<T>((const void*)trti2_batched_kernel<T, kDiagThreads>, sizeof(T) * nb * nb));
-  trti2_batched_kernel<T, kDiagThreads><<<1, kDiagThreads, sizeof(T) * n * n, stream>>>(B, brs, bcs, n, n,
-                                                                                      unit ? 1 : 0);
+  constexpr int NB = Tune<T>::nb;
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_invert_kernel<T, NB, kDiagThreads2>, DiagSmem<T, NB>::bytes));
+  diag_invert_kernel<T, NB, kDiagThreads2><<<1, kDiagThreads2, DiagSmem<T, NB>::bytes, stream>>>(
+      B, brs, bcs, n, n, unit ? 1 : 0);
   ++h->launches;
   CUCHOL_CHECK(cudaGetLastError());
   return CUDA_SUCCESS;
@@ -422,6 +556,10 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   if (h == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
   memset(h, 0, sizeof(*h));
   CUCHOL_CHECK(cudaGetDevice(&h->device));
+  {
+    const char* e = getenv("CUCHOLESKY_FORCE_SIMT");   // testing: FP64 products on the SIMT engine
+    h->force_simt = (e != nullptr && e[0] == '1') ? 1 : 0;
+  }
   CUCHOL_CHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
   int lo = 0, hi = 0;
   CUCHOL_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -431,6 +569,7 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_panel, cudaEventDisableTiming));
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_update, cudaEventDisableTiming));
   CUCHOL_CHECK(cudaMalloc(&h->d_words, 16 * sizeof(int)));
+  CUCHOL_CHECK(cudaMemset(h->d_words, 0, 16 * sizeof(int)));
   CUCHOL_CHECK(cudaMallocHost(&h->h_words, 16 * sizeof(int)));
   CUCHOL_CHECK(cudaMalloc(&h->d_logdet, 4 * sizeof(double)));
   CUCHOL_CHECK(cudaMalloc(&h->d_logdet_f, 4 * sizeof(float)));
@@ -615,3 +754,150 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKGetLaunchCount(CULAPACKhandle h, unsig
   *count = h->launches;
   return CUDA_SUCCESS;
 }
+
+// ------------------------------------------------------------------------------
+// BLAS layer (include/blas.h): cu?gemm2, cu?syrk, cu?herk on the same engines,
+// queued on the caller's stream.  Argument checks follow blas/dgemm.c:154-171,
+// blas/dsyrk.c:166-179 and blas/zherk.c:190-205.
+// ------------------------------------------------------------------------------
+struct __cublashandle_st {
+  CULAPACKhandle lh;
+};
+
+extern "C" CUCHOL_EXPORT CUresult cuBLASCreate(CUBLAShandle* handle) {
+  if (handle == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  auto* b = new (std::nothrow) __cublashandle_st;
+  if (b == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
+  CUresult r = cuLAPACKCreate(&b->lh);
+  if (r != CUDA_SUCCESS) {
+    delete b;
+    return r;
+  }
+  *handle = b;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuBLASDestroy(CUBLAShandle b) {
+  if (b == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  CUresult r = cuLAPACKDestroy(b->lh);
+  delete b;
+  return r;
+}
+
+namespace {
+
+template <typename T>
+bool eq(const T& a, RealOf<T> r) {
+  if constexpr (Traits<T>::complex) return a.x == r && a.y == 0;
+  else return a == r;
+}
+
+// Operand view of op(X) as "rows x k" (rows_first) or "k x rows" (for B).
+template <typename T>
+void view_a(GemmProblem<T>& p, CBlasTranspose tr, CUdeviceptr A, size_t lda) {
+  p.a = reinterpret_cast<const T*>(A);
+  if (tr == CBlasNoTrans) { p.a_rs = 1; p.a_ks = (long long)lda; }
+  else { p.a_rs = (long long)lda; p.a_ks = 1; p.conj_a = (tr == CBlasConjTrans); }
+}
+template <typename T>
+void view_b(GemmProblem<T>& p, CBlasTranspose tr, CUdeviceptr B, size_t ldb) {
+  p.b = reinterpret_cast<const T*>(B);
+  if (tr == CBlasNoTrans) { p.b_rs = (long long)ldb; p.b_ks = 1; }
+  else { p.b_rs = 1; p.b_ks = (long long)ldb; p.conj_b = (tr == CBlasConjTrans); }
+}
+
+inline bool bad_trans(CBlasTranspose t) { return t != CBlasNoTrans && t != CBlasTrans && t != CBlasConjTrans; }
+
+template <typename T>
+CUresult api_gemm2(const char* name, CUBLAShandle bh, CBlasTranspose ta, CBlasTranspose tb, size_t m, size_t n,
+                   size_t k, T alpha, CUdeviceptr A, size_t lda, CUdeviceptr B, size_t ldb, T beta, CUdeviceptr C,
+                   size_t ldc, CUdeviceptr D, size_t ldd, CUstream stream) {
+  const size_t nRowA = (ta == CBlasNoTrans) ? m : k;
+  const size_t nRowB = (tb == CBlasNoTrans) ? k : n;
+  int info = 0;
+  if (lda < nRowA) info = 8;
+  else if (ldb < nRowB) info = 10;
+  else if (ldc < m) info = 13;
+  else if (ldd < m) info = 15;
+  if (info != 0) {
+    if (xerbla != nullptr) xerbla(name, info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (m == 0 || n == 0 || (C == D && ldc == ldd && (eq(alpha, 0) || k == 0) && eq(beta, 1))) return CUDA_SUCCESS;
+  if (bh == nullptr || bad_trans(ta) || bad_trans(tb) || m > INT_MAX || n > INT_MAX || k > INT_MAX)
+    return CUDA_ERROR_INVALID_VALUE;
+  GemmProblem<T> p = problem<T>();
+  view_a<T>(p, ta, A, lda);
+  view_b<T>(p, tb, B, ldb);
+  p.c = reinterpret_cast<T*>(D); p.c_rs = 1; p.c_cs = (long long)ldd;
+  if (!eq(beta, 0)) { p.cin = reinterpret_cast<const T*>(C); p.cin_rs = 1; p.cin_cs = (long long)ldc; }
+  p.alpha = alpha; p.beta = beta;
+  p.m = (int)m; p.n = (int)n; p.k = (int)k;
+  if (k == 0 || eq(alpha, 0)) { p.k = 0; }
+  return gemm<T>(bh->lh, p, reinterpret_cast<cudaStream_t>(stream), nullptr);
+}
+
+// C := alpha op(A) op(A)^H + beta C on one triangle (herk: alpha, beta real; syrk: the
+// transpose without conjugation).
+template <typename T>
+CUresult api_rankk(const char* name, bool herm, CUBLAShandle bh, CBlasUplo uplo, CBlasTranspose tr, size_t n,
+                   size_t k, RealOf<T> alpha, CUdeviceptr A, size_t lda, RealOf<T> beta, CUdeviceptr C, size_t ldc,
+                   CUstream stream) {
+  const size_t nRowA = (tr == CBlasNoTrans) ? n : k;
+  int info = 0;
+  if (herm && tr == CBlasTrans) info = 2;
+  else if (lda < nRowA) info = 7;
+  else if (ldc < n) info = 10;
+  if (info != 0) {
+    if (xerbla != nullptr) xerbla(name, info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (n == 0 || ((alpha == 0 || k == 0) && beta == 1)) return CUDA_SUCCESS;
+  if (bh == nullptr || bad_uplo(uplo) || bad_trans(tr) || n > INT_MAX || k > INT_MAX)
+    return CUDA_ERROR_INVALID_VALUE;
+  GemmProblem<T> p = problem<T>();
+  const CBlasTranspose t2 = (tr == CBlasNoTrans) ? CBlasNoTrans : CBlasTrans;
+  view_a<T>(p, t2, A, lda);
+  p.b = p.a; p.b_rs = p.a_rs; p.b_ks = p.a_ks;
+  if (herm) {
+    // lower: A A^H (N) or A^H A (C); the upper triangle is the lower triangle of
+    // the conjugate, read through the transposed view of C
+    const bool cA = (tr != CBlasNoTrans);
+    p.conj_a = cA; p.conj_b = !cA;
+    if (uplo == CBlasUpper) { p.conj_a = !p.conj_a; p.conj_b = !p.conj_b; }
+    p.real_diag = 1;
+  }
+  if (uplo == CBlasLower) { p.c_rs = 1; p.c_cs = (long long)ldc; }
+  else { p.c_rs = (long long)ldc; p.c_cs = 1; }
+  p.c = reinterpret_cast<T*>(C);
+  if (beta != 0) { p.cin = p.c; p.cin_rs = p.c_rs; p.cin_cs = p.c_cs; }
+  p.alpha = from_real<T>(alpha); p.beta = from_real<T>(beta);
+  p.lower_only = 1;
+  p.m = (int)n; p.n = (int)n; p.k = (alpha == 0) ? 0 : (int)k;
+  return gemm<T>(bh->lh, p, reinterpret_cast<cudaStream_t>(stream), nullptr);
+}
+
+}  // namespace
+
+#define CUCHOL_API_GEMM(P, T)                                                                                   \
+  extern "C" CUCHOL_EXPORT CUresult cu##P##gemm2(CUBLAShandle h, CBlasTranspose ta, CBlasTranspose tb, size_t m, \
+                                                 size_t n, size_t k, T alpha, CUdeviceptr A, size_t lda,        \
+                                                 CUdeviceptr B, size_t ldb, T beta, CUdeviceptr C, size_t ldc,  \
+                                                 CUdeviceptr D, size_t ldd, CUstream s) {                       \
+    return api_gemm2<T>("cu" #P "gemm2", h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, D, ldd, s);  \
+  }
+CUCHOL_API_GEMM(S, float)
+CUCHOL_API_GEMM(D, double)
+CUCHOL_API_GEMM(C, cuFloatComplex)
+CUCHOL_API_GEMM(Z, cuDoubleComplex)
+
+#define CUCHOL_API_RANKK(NAME, T, HERM)                                                                         \
+  extern "C" CUCHOL_EXPORT CUresult NAME(CUBLAShandle h, CBlasUplo u, CBlasTranspose tr, size_t n, size_t k,   \
+                                         RealOf<T> alpha, CUdeviceptr A, size_t lda, RealOf<T> beta,            \
+                                         CUdeviceptr C, size_t ldc, CUstream s) {                               \
+    return api_rankk<T>(#NAME, HERM, h, u, tr, n, k, alpha, A, lda, beta, C, ldc, s);                          \
+  }
+CUCHOL_API_RANKK(cuSsyrk, float, false)
+CUCHOL_API_RANKK(cuDsyrk, double, false)
+CUCHOL_API_RANKK(cuCherk, cuFloatComplex, true)
+CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)

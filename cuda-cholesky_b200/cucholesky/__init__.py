@@ -69,9 +69,10 @@ def _declare(L: C.CDLL) -> None:
 
 def exported_symbols() -> list[str]:
     """Names a C caller links against (the include/lapack.h prototypes)."""
-    names = ["cuLAPACKCreate", "cuLAPACKDestroy", "xerbla", "errorHandler"]
+    names = ["cuLAPACKCreate", "cuLAPACKDestroy", "xerbla", "errorHandler", "cuBLASCreate", "cuBLASDestroy",
+             "cuSsyrk", "cuDsyrk", "cuCherk", "cuZherk"]
     for p in "SDCZ":
-        names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet")]
+        names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet", "gemm2")]
     return names
 
 
@@ -205,3 +206,85 @@ def logdet_of_factor(h: Handle, T, n: int) -> float:
         raise CuCholeskyError(f"cu{_prefix(T)}logdet", rc)
     torch.cuda.synchronize()
     return float(out.value)
+
+
+# ---- BLAS layer (include/blas.h) -------------------------------------------------
+
+class _CF(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class _CD(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double)]
+
+
+_SCAL = {"S": C.c_float, "D": C.c_double, "C": _CF, "Z": _CD}
+_REAL = {"S": C.c_float, "D": C.c_double, "C": C.c_float, "Z": C.c_double}
+
+
+def _declare_blas(L: C.CDLL) -> None:
+    L.cuBLASCreate.argtypes = [C.POINTER(C.c_void_p)]
+    L.cuBLASCreate.restype = C.c_int
+    L.cuBLASDestroy.argtypes = [C.c_void_p]
+    L.cuBLASDestroy.restype = C.c_int
+    for p in "SDCZ":
+        f = getattr(L, f"cu{p}gemm2")
+        S = _SCAL[p]
+        f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, S, C.c_uint64, C.c_size_t,
+                      C.c_uint64, C.c_size_t, S, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t, C.c_void_p]
+        f.restype = C.c_int
+    for name, p in (("cuSsyrk", "S"), ("cuDsyrk", "D"), ("cuCherk", "C"), ("cuZherk", "Z")):
+        f = getattr(L, name)
+        R = _REAL[p]
+        f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_size_t, R, C.c_uint64, C.c_size_t, R,
+                      C.c_uint64, C.c_size_t, C.c_void_p]
+        f.restype = C.c_int
+
+
+class BlasHandle:
+    """CUBLAShandle of this library (not NVIDIA cuBLAS)."""
+
+    def __init__(self):
+        L = lib()
+        if not getattr(L, "_blas_declared", False):
+            _declare_blas(L)
+            L._blas_declared = True
+        self._h = C.c_void_p()
+        rc = L.cuBLASCreate(C.byref(self._h))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuBLASCreate", rc)
+
+    @property
+    def value(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().cuBLASDestroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _scal(p: str, v):
+    if p in "CZ":
+        v = complex(v)
+        return _SCAL[p](v.real, v.imag)
+    return _SCAL[p](v)
+
+
+def call_gemm2(bh: BlasHandle, p: str, ta: str, tb: str, m: int, n: int, k: int, alpha, a: int, lda: int,
+               b: int, ldb: int, beta, c: int, ldc: int, d: int, ldd: int, stream: int = 0) -> int:
+    return getattr(lib(), f"cu{p}gemm2")(bh.value, ord(ta), ord(tb), m, n, k, _scal(p, alpha), a, lda, b, ldb,
+                                         _scal(p, beta), c, ldc, d, ldd, C.c_void_p(stream))
+
+
+def call_rankk(bh: BlasHandle, p: str, uplo: str, trans: str, n: int, k: int, alpha: float, a: int, lda: int,
+               beta: float, c: int, ldc: int, stream: int = 0) -> int:
+    name = {"S": "cuSsyrk", "D": "cuDsyrk", "C": "cuCherk", "Z": "cuZherk"}[p]
+    return getattr(lib(), name)(bh.value, ord(uplo), ord(trans), n, k, _REAL[p](alpha), a, lda, _REAL[p](beta),
+                                c, ldc, C.c_void_p(stream))

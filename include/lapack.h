@@ -28,31 +28,11 @@
 #ifndef CUCHOLESKY_LAPACK_H
 #define CUCHOLESKY_LAPACK_H
 
-#include <stddef.h>
-#include <cuda.h>
+#include "blas.h"
 
 #ifdef __cplusplus
 extern "C" {
 #endif
-
-/* BLAS enums, castable to char (reference include/blas.h:24-27). */
-#ifndef CUCHOLESKY_NO_CBLAS_ENUMS
-typedef enum { CBlasNoTrans = 'N', CBlasTrans = 'T', CBlasConjTrans = 'C' } CBlasTranspose;
-typedef enum { CBlasLower = 'L', CBlasUpper = 'U' } CBlasUplo;
-typedef enum { CBlasLeft = 'L', CBlasRight = 'R' } CBlasSide;
-typedef enum { CBlasNonUnit = 'N', CBlasUnit = 'U' } CBlasDiag;
-#endif
-
-/* Argument-error hook (reference include/blas.h:39-44, blas/xerbla.c:9).  Called
- * with the routine name and the 1-based position of the bad argument; may be set
- * to NULL or replaced by the caller. */
-typedef void (*xerbla_t)(const char *, long);
-extern xerbla_t xerbla;
-
-/* CUDA error hook (reference include/error.h:23-32, multigpu/error.c:11). */
-typedef void (*errorHandler_t)(const char *, const char *, const char *, int,
-                               int, const char * (*)(int));
-extern errorHandler_t errorHandler;
 
 /* Handle: binds the device current at creation, owns streams, events and cached
  * device workspace (reference include/lapack.h:63-65, lapack/handle.c:77-88).
