@@ -76,8 +76,6 @@ namespace {
 
 __global__ void narrow_double_kernel(const double* s, float* d) { *d = (float)*s; }
 
-constexpr int kDiagThreads = 512;
-
 template <typename T> struct Tune { static constexpr int nb = 128; };
 template <> struct Tune<cuDoubleComplex> { static constexpr int nb = 64; };
 
