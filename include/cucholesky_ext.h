@@ -24,6 +24,28 @@ CUresult cuCpotrfLogdet(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, 
  * measurement; counts this library's own kernels only). */
 CUresult cuLAPACKGetLaunchCount(CULAPACKhandle, unsigned long long *);
 
+/* log det from a strided FP64 diagonal, 2 * sum_i log(x[i*incx]), for callers that
+ * cannot allocate device memory.  No counterpart in the reference library.
+ *
+ * Who needs it: cuDlogdet keeps its scratch in a handle that cuLAPACKCreate
+ * allocates with cudaMalloc (and the reference's cuDlogdet allocates and frees
+ * on every call).  Some callers may not do that: code whose device memory is owned
+ * by another allocator (a framework's caching allocator or a pool reserved at
+ * start-up, where a cudaMalloc outside it fails or fragments the budget), and
+ * loops that must not allocate or free after start-up because cudaFree can
+ * synchronise the whole device.  This entry point takes no handle and calls no
+ * cudaMalloc, cudaFree or other allocating routine: its scratch is a static device
+ * array of about 32 KB that every GPU loading the library holds until exit.
+ *
+ * Limit: n <= 8,388,608 (the array holds one partial sum per 2048 elements);
+ * larger n calls XERBLA with position 3 and returns CUDA_ERROR_INVALID_VALUE.
+ * The work is queued on `stream`; *result is valid once the stream has
+ * synchronised.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current, so make that first
+ * call before any stream capture.  All calls share the one array and each call
+ * clears what must start at zero: calls that overlap on the GPU race. */
+CUresult cuDlogdetNoAlloc(CUdeviceptr x, size_t incx, size_t n, double *result, CUstream stream);
+
 #ifdef __cplusplus
 }
 #endif
