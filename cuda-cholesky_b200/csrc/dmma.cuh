@@ -4,8 +4,10 @@
 // DMMA instruction mma.sync.aligned.m16n8k4.row.col.f64 (measured on B200: 37.1
 // TFLOP/s device-wide, the same rate as DFMA).  Operand tiles are staged into
 // shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle, no multicast)
-// through a 4-stage ring driven by mbarriers: one producer warp issues the copies,
-// four consumer warps (2 x 2, 64 x 32 each) run the MMAs on a 128 x 64 tile.
+// through a 4-stage ring: thread 0 issues the copies (completion tracked by one
+// mbarrier per stage), and the CTA's four warps (2 x 2, 64 x 32 each) run the MMAs
+// on a 128 x 64 tile.  No dedicated producer warp: with 4 warps of at most 255
+// registers two CTAs fit on an SM, so 8 MMA warps hide each other's latency.
 //
 // Problem form: the GemmProblem of gemm.cuh for T = double,
 //     C(i, j) = alpha * sum_k Ahat(i, k) * Bhat(j, k) + beta * Cin(i, j),
@@ -32,8 +34,8 @@ namespace cuchol {
 namespace dmma {
 
 constexpr int BM = 128, BN = 64, BK = 16, STAGES = 4;
-constexpr int CONSUMERS = 4;                       // 2 x 2 warps of 64 x 32
-constexpr int THREADS = (CONSUMERS + 1) * 32;
+constexpr int WARPS = 4;                           // 2 x 2 warps of 64 x 32
+constexpr int THREADS = WARPS * 32;
 constexpr int A_STAGE = BM * BK * 8;               // 16 KB
 constexpr int B_STAGE = BN * BK * 8;               // 8 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
@@ -66,9 +68,6 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -120,7 +119,7 @@ __device__ __forceinline__ double tri_mask(double v, int tri, int unit, int row,
 }
 
 template <int LA, int LB, bool TRI>
-__global__ void __maxnreg__(200)
+__global__ void __launch_bounds__(THREADS, 2)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
   if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
@@ -141,42 +140,28 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], CONSUMERS);
-    }
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full_bar[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  // thread 0 fills the ring: stage kt % STAGES holds k block kt
+  auto issue = [&](int kt) {
+    const int s = kt % STAGES;
+    unsigned char* st = smem + s * STAGE_BYTES;
+    mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+    load_operand<LA, BM>(&mapA, &full_bar[s], st, i0, kbase + kt * BK);
+    load_operand<LB, BN>(&mapB, &full_bar[s], st + A_STAGE, j0, kbase + kt * BK);
+  };
+  int issued = 0;
+  if (threadIdx.x == 0)
+    for (; issued < KT && issued < STAGES; ++issued) issue(issued);
 
-  if (warp == CONSUMERS) {
-    // ---------------- producer ----------------
-    if (lane == 0) {
-      int issued = 0;
-      bool ok = true;
-      for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt % STAGES;
-        if (kt >= STAGES && !mbar_wait(&empty_bar[s], ((kt / STAGES) - 1) & 1)) { ok = false; break; }
-        unsigned char* st = smem + s * STAGE_BYTES;
-        mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-        load_operand<LA, BM>(&mapA, &full_bar[s], st, i0, kbase + kt * BK);
-        load_operand<LB, BN>(&mapB, &full_bar[s], st + A_STAGE, j0, kbase + kt * BK);
-        issued = kt + 1;
-      }
-      if (!ok) atomicExch(P.err, 1);
-      // every issued copy must have landed before the CTA may exit
-      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
-        if (!mbar_wait(&full_bar[kt % STAGES], (kt / STAGES) & 1)) atomicExch(P.err, 2);
-    }
-    return;
-  }
-
-  // ---------------- consumers ----------------
+  // ---------------- MMA warps ----------------
   const int wm = warp & 1, wn = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
   const int fg = fperm(g);
@@ -245,7 +230,9 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   bool ok = true;
   for (int kt = 0; kt < KT; ++kt) {
     const int s = kt % STAGES;
-    if (!mbar_wait(&full_bar[s], (kt / STAGES) & 1)) { ok = false; break; }
+    // bounded wait; the give-up decision is made CTA-uniform at the barrier below
+    const bool got = mbar_wait(&full_bar[s], (kt / STAGES) & 1);
+    if (got) {
     const unsigned char* As = smem + s * STAGE_BYTES;
     const unsigned char* Bs = As + A_STAGE;
     const int ks = kbase + kt * BK;
@@ -345,11 +332,21 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
       }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty_bar[s]);
+    }   // got
+    // every warp is done with stage s: refill it with k block kt + STAGES
+    if (!__syncthreads_and(got)) {
+      ok = false;
+      break;
+    }
+    if (threadIdx.x == 0 && issued < KT) issue(issued++);
   }
   if (!ok) {
+    // a wait gave up: record it, and let thread 0 wait (bounded) for the copies it
+    // issued before the CTA exits
     if (lane == 0) atomicExch(P.err, 3);
+    if (threadIdx.x == 0)
+      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
+        mbar_wait(&full_bar[kt % STAGES], (kt / STAGES) & 1);
     return;
   }
 

@@ -148,6 +148,9 @@ CUresult launch_dmma(CULAPACKhandle h, const CUtensorMap& ma, const CUtensorMap&
   if (!attr) {
     CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       dmma::SMEM_BYTES));
+    // two CTAs per SM: ask for the whole unified L1/shared carve-out
+    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     attr = true;
   }
   dmma::gemm_kernel<LA, LB, TRI><<<tiles, dmma::THREADS, dmma::SMEM_BYTES, s>>>(ma, mb, q, abort);
