@@ -72,99 +72,98 @@ __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
 
 // Warp: Cholesky of the pb x pb sub-block at (c0, c0) of S, lower part, in place.
-// Lane i keeps the not yet factored part of row i in registers as a window that
-// shifts left by one column per pivot, so the loop body is the same for every
-// pivot (compact code: it runs once per launch and must not stream a long unrolled
-// sequence through a cold instruction cache).  rdiag[c0+k] = 1 / L(k,k).
-// Returns the first failing local column (pivot <= 0 or NaN) or -1; on failure
-// the factored columns are in S and the failing pivot is left as updated.
+// (The three warp routines are not inlined: compiled as separate functions each
+// keeps its 32-element array in registers.)
+// Lane i holds row i in registers; both loops are unrolled so every index is a
+// compile-time register name (no window shifting): per pivot, one shuffle of the
+// pivot, one rsqrt, then 31-k independent shuffle + FMA pairs.  rdiag[c0+k] =
+// 1 / L(k,k).  Returns the first failing local column (pivot <= 0 or NaN) or -1;
+// on failure the columns before it are factored and the rest is left as updated.
 template <typename T>
-__device__ int warp_chol32(T* S, int LD, int c0, int pb, T* rdiag) {
+__device__ __noinline__ int warp_chol32(T* S, int LD, int c0, int pb, T* rdiag) {
   using R = RealOf<T>;
   const int i = threadIdx.x & 31;
-  T a[32];   // a[t] = current A(i, k + t)
+  T a[32];
 #pragma unroll
-  for (int t = 0; t < 32; ++t) a[t] = (i < pb && t <= i) ? S[(c0 + t) * LD + c0 + i] : zero<T>();
+  for (int j = 0; j < 32; ++j) a[j] = (i < pb && j <= i) ? S[(c0 + j) * LD + c0 + i] : zero<T>();
   int fail = -1;
-  for (int k = 0; k < pb; ++k) {
-    const R d = re(shfl(a[0], k));
-    if (!(d > R(0))) {   // warp-uniform
-      fail = k;
-      if (i == k) S[(c0 + k) * LD + c0 + k] = a[0];
-      break;
-    }
-    const R r = rsqrt_(d);
-    T l = scale(a[0], r);                 // L(i, k) for i > k
-    if (i == k) {
-      l = from_real<T>(d * r);            // L(k, k) = sqrt(d)
-      rdiag[c0 + k] = from_real<T>(r);
-    }
-    if (i >= k && i < pb) S[(c0 + k) * LD + c0 + i] = l;
-    // A(i, k+t) -= L(i, k) conj(L(k+t, k)),  t >= 1, k + t <= i
 #pragma unroll
-    for (int t = 1; t < 32; ++t) {
-      const T lt = shfl(l, (k + t) & 31);
-      if (i >= k + t) mac(a[t], neg(l), cj(lt));
-    }
+  for (int k = 0; k < 32; ++k) {
+    if (k < pb && fail < 0) {                     // warp-uniform
+      const R d = re(shfl(a[k], k));
+      if (!(d > R(0))) {
+        fail = k;
+      } else {
+        const R r = rsqrt_(d);
+        const T l = (i == k) ? from_real<T>(d * r) : scale(a[k], r);
+        if (i == k) rdiag[c0 + k] = from_real<T>(r);
 #pragma unroll
-    for (int t = 0; t < 31; ++t) a[t] = a[t + 1];
-    a[31] = zero<T>();
+        for (int j = k + 1; j < 32; ++j) {
+          const T lj = shfl(l, j);
+          if (i >= j) mac(a[j], neg(l), cj(lj));
+        }
+        if (i >= k) a[k] = l;
+      }
+    }
   }
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    if (i < pb && j <= i) S[(c0 + j) * LD + c0 + i] = a[j];
   __syncwarp();
   return fail;
 }
 
-// Rows [r0, r1) of sub-block column c0: solve x L_pp^H = b in place (one thread per
-// row, forward substitution with a shifting register window):
-//   x_j = b_j / L(j,j);  b_{j+t} -= x_j conj(L(j+t, j)).
+// Rows [r0, r1) of sub-block column c0: solve x L_pp^H = b in place, one thread per
+// row, unrolled forward substitution (L read from shared memory by broadcast):
+//   x_j = (b_j - sum_{k<j} x_k conj(L(j,k))) conj(1/L(j,j)).
 template <typename T, int NT>
-__device__ void rows_solve(T* S, int LD, int c0, int pb, int r0, int r1, const T* rdiag) {
+__device__ __noinline__ void rows_solve(T* S, int LD, int c0, int pb, int r0, int r1, const T* rdiag) {
   for (int r = r0 + threadIdx.x; r < r1; r += NT) {
-    T b[32];
+    T x[32];
 #pragma unroll
-    for (int t = 0; t < 32; ++t) b[t] = (t < pb) ? S[(c0 + t) * LD + r] : zero<T>();
-    for (int j = 0; j < pb; ++j) {
-      const T x = mul(b[0], cj(rdiag[c0 + j]));
-      S[(c0 + j) * LD + r] = x;
-      const T* lc = S + (c0 + j) * LD + c0 + j;   // L(j + t, j) = lc[t]
+    for (int j = 0; j < 32; ++j) x[j] = (j < pb) ? S[(c0 + j) * LD + r] : zero<T>();
 #pragma unroll
-      for (int t = 1; t < 32; ++t)
-        if (j + t < pb) mac(b[t], neg(x), cj(lc[t]));
+    for (int j = 0; j < 32; ++j) {
+      if (j < pb) {
+        T s0 = x[j], s1 = zero<T>();
 #pragma unroll
-      for (int t = 0; t < 31; ++t) b[t] = b[t + 1];
-      b[31] = zero<T>();
+        for (int k = 0; k < j; ++k) {
+          const T l = cj(S[(c0 + k) * LD + c0 + j]);
+          if (k & 1) mac(s1, neg(x[k]), l); else mac(s0, neg(x[k]), l);
+        }
+        x[j] = mul(add(s0, s1), cj(rdiag[c0 + j]));
+      }
     }
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j < pb) S[(c0 + j) * LD + r] = x[j];
   }
 }
 
 // Warp: X = inv(L_pp) for the pb x pb lower sub-block at (c0, c0) (unit: implicit
-// unit diagonal; rdiag[c0+i] = 1/L(i,i) otherwise).  Lane j computes column j:
-//   X(j,j) = 1/L(j,j),  X(i,j) = -(1/L(i,i)) sum_{k=j..i-1} L(i,k) X(k,j),
-// with four partial sums per dot product.  X(i, j) is stored at X[j*33 + i]:
-// lower part written, upper part zero.
+// unit diagonal; rdiag[c0+i] = 1/L(i,i) otherwise).  Lane j computes column j in
+// registers, unrolled:
+//   X(j,j) = 1/L(j,j),  X(i,j) = -(1/L(i,i)) sum_{k=j..i-1} L(i,k) X(k,j).
+// X(i, j) is stored at X[j*33 + i]: lower part written, upper part zero.
 template <typename T>
-__device__ void warp_inv32(const T* S, int LD, int c0, int pb, const T* rdiag, bool unit, T* X) {
+__device__ __noinline__ void warp_inv32(const T* S, int LD, int c0, int pb, const T* rdiag, bool unit, T* X) {
   const int j = threadIdx.x & 31;
-  T* xj = X + j * 33;
-  for (int i = 0; i < 32; ++i) {
-    T v = zero<T>();
-    if (j < pb && i < pb && i >= j) {
-      const T ri = unit ? from_real<T>(RealOf<T>(1)) : rdiag[c0 + i];
-      if (i == j) {
-        v = ri;
-      } else {
-        T s[4] = {zero<T>(), zero<T>(), zero<T>(), zero<T>()};
-        int k = j;
-        for (; k + 3 < i; k += 4) {
+  T x[32];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) mac(s[q], S[(c0 + k + q) * LD + c0 + i], xj[k + q]);
-        }
-        for (; k < i; ++k) mac(s[0], S[(c0 + k) * LD + c0 + i], xj[k]);
-        v = neg(mul(ri, add(add(s[0], s[1]), add(s[2], s[3]))));
+  for (int i = 0; i < 32; ++i) {
+    const T ri = unit ? from_real<T>(RealOf<T>(1)) : (i < pb ? rdiag[c0 + i] : zero<T>());
+    T s0 = zero<T>(), s1 = zero<T>();
+#pragma unroll
+    for (int k = 0; k < i; ++k) {
+      if (k >= j) {
+        const T l = S[(c0 + k) * LD + c0 + i];
+        if (k & 1) mac(s1, l, x[k]); else mac(s0, l, x[k]);
       }
     }
-    xj[i] = v;
+    x[i] = (i < j || i >= pb || j >= pb) ? zero<T>() : (i == j ? ri : neg(mul(ri, add(s0, s1))));
   }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) X[j * 33 + i] = x[i];
 }
 
 // S(r, c) -= sum_{k < c0} S(r, k) conj(S(c, k)) for rows [c0, nr), columns
@@ -180,6 +179,7 @@ __device__ void block_update(T* S, int LD, int c0, int pb, int nr) {
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[u][v] = zero<T>();
+#pragma unroll 4
     for (int k = 0; k < c0; ++k) {
       T a[4], b[4];
 #pragma unroll
@@ -214,6 +214,7 @@ __device__ void inverse_offdiag(T* S, int LD, int r0, int nr, int c0, int nc, T*
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[u][v] = zero<T>();
+#pragma unroll 4
     for (int k = cb; k < nc; ++k) {
       T a[4], b[4];
 #pragma unroll
@@ -240,6 +241,7 @@ __device__ void inverse_offdiag(T* S, int LD, int r0, int nr, int c0, int nc, T*
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[u][v] = zero<T>();
+#pragma unroll 4
     for (int k = 0; k < min(nr, rb + 4); ++k) {
       T a[4], b[4];
 #pragma unroll
