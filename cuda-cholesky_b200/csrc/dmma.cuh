@@ -51,7 +51,7 @@ struct Params {
   double alpha, beta;
   int tri_a, tri_b, unit_a, unit_b;
   int lower_only;
-  int tiles_n;
+  int tiles_m, tiles_n;
   int vec_ok;            // C / Cin 16-byte aligned along their unit stride, Cin == C
   int preload;           // alpha = +-1: accumulators start at beta*Cin (loaded before
                          // the k loop, so its latency hides under the TMA fill)
@@ -123,19 +123,25 @@ __global__ void __launch_bounds__(THREADS, 2)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
   if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
-  const int tile = blockIdx.x;
-  const int ti = tile / P.tiles_n, tj = tile % P.tiles_n;
-  const int i0 = ti * BM, j0 = tj * BN;
-  if (P.lower_only && j0 > i0 + BM - 1) return;
-
-  // k range of this tile (triangular views limit it), aligned down to BK
-  int kb = 0, ke = P.k;
-  if (P.tri_a == TRI_LOWER) ke = min(ke, i0 + BM);
-  if (P.tri_a == TRI_UPPER) kb = max(kb, i0);
-  if (P.tri_b == TRI_LOWER) ke = min(ke, j0 + BN);
-  if (P.tri_b == TRI_UPPER) kb = max(kb, j0);
-  const int kbase = (kb / BK) * BK;
-  const int KT = (ke > kbase) ? (ke - kbase + BK - 1) / BK : 0;
+  // This CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...  The host picks the
+  // grid so that a CTA handles several tiles: the TMA ring keeps streaming across
+  // tile boundaries, while CTAs still retire often enough for other streams' kernels.
+  const int ntiles = P.tiles_m * P.tiles_n;
+  // rows i0, columns j0 and k range [kbase, kbase + KT*BK) of a tile (triangular
+  // views limit it); false for a tile wholly above the diagonal of a lower-only output
+  auto tile_range = [&](int tile, int& i0, int& j0, int& kbase, int& KT) -> bool {
+    i0 = (tile / P.tiles_n) * BM;
+    j0 = (tile % P.tiles_n) * BN;
+    if (P.lower_only && j0 > i0 + BM - 1) return false;
+    int kb = 0, ke = P.k;
+    if (P.tri_a == TRI_LOWER) ke = min(ke, i0 + BM);
+    if (P.tri_a == TRI_UPPER) kb = max(kb, i0);
+    if (P.tri_b == TRI_LOWER) ke = min(ke, j0 + BN);
+    if (P.tri_b == TRI_UPPER) kb = max(kb, j0);
+    kbase = (kb / BK) * BK;
+    KT = (ke > kbase) ? (ke - kbase + BK - 1) / BK : 0;
+    return true;
+  };
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem =
@@ -149,17 +155,29 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
-  // thread 0 fills the ring: stage kt % STAGES holds k block kt
-  auto issue = [&](int kt) {
-    const int s = kt % STAGES;
+  // Thread 0 fills the ring in the order the tiles consume it: item q (the q-th
+  // k block of this CTA, over all its tiles) goes to stage q % STAGES.
+  int p_tile = (int)blockIdx.x - (int)gridDim.x, p_kt = 0, p_KT = 0, p_i0 = 0, p_j0 = 0, p_kbase = 0;
+  long long issued = 0, consumed = 0;
+  auto produce = [&]() -> bool {   // issue the next item; false when none is left
+    while (p_kt >= p_KT) {
+      p_tile += gridDim.x;
+      if (p_tile >= ntiles) return false;
+      p_kt = 0;
+      if (!tile_range(p_tile, p_i0, p_j0, p_kbase, p_KT)) p_KT = 0;
+    }
+    const int s = (int)(issued % STAGES);
     unsigned char* st = smem + s * STAGE_BYTES;
     mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-    load_operand<LA, BM>(&mapA, &full_bar[s], st, i0, kbase + kt * BK);
-    load_operand<LB, BN>(&mapB, &full_bar[s], st + A_STAGE, j0, kbase + kt * BK);
+    load_operand<LA, BM>(&mapA, &full_bar[s], st, p_i0, p_kbase + p_kt * BK);
+    load_operand<LB, BN>(&mapB, &full_bar[s], st + A_STAGE, p_j0, p_kbase + p_kt * BK);
+    ++p_kt;
+    ++issued;
+    return true;
   };
-  int issued = 0;
   if (threadIdx.x == 0)
-    for (; issued < KT && issued < STAGES; ++issued) issue(issued);
+    for (int q = 0; q < STAGES && produce(); ++q) {
+    }
 
   // ---------------- MMA warps ----------------
   const int wm = warp & 1, wn = warp >> 1;
@@ -169,6 +187,10 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   // of its B fragment inside an n8 block, per layout
   const int arow0 = (LA == LAYOUT_R) ? 2 * g : fg;
   const int arow1 = (LA == LAYOUT_R) ? 2 * g + 1 : fg + 8;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  int i0, j0, kbase, KT;
+  if (!tile_range(tile, i0, j0, kbase, KT)) continue;
   double acc[4][4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -227,11 +249,10 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
     }
   }
-  bool ok = true;
-  for (int kt = 0; kt < KT; ++kt) {
-    const int s = kt % STAGES;
+  for (int kt = 0; kt < KT; ++kt, ++consumed) {
+    const int s = (int)(consumed % STAGES);
     // bounded wait; the give-up decision is made CTA-uniform at the barrier below
-    const bool got = mbar_wait(&full_bar[s], (kt / STAGES) & 1);
+    const bool got = mbar_wait(&full_bar[s], (unsigned)((consumed / STAGES) & 1));
     if (got) {
     const unsigned char* As = smem + s * STAGE_BYTES;
     const unsigned char* Bs = As + A_STAGE;
@@ -289,6 +310,38 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 #pragma unroll
         for (int v = 0; v < 4; ++v) bv[v] = make_double2(-bv[v].x, -bv[v].y);
       }
+      if constexpr (LA == LAYOUT_R) {
+        // step-major order: an accumulator is reused only after the 15 other MMAs
+        // of the step, so back-to-back MMAs never depend on each other
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+          const int k = q * 8 + 2 * t + s2;
+          double2 av[4];
+#pragma unroll
+          for (int mb = 0; mb < 4; ++mb) {
+            const unsigned char* box = As + (wm * 4 + mb) * 2048;
+            av[mb] = *reinterpret_cast<const double2*>(box + k * 128 + ((g ^ (k & 7)) << 4));
+            if (mask_a) {
+              const int ra = wrow + mb * 16;
+              av[mb].x = tri_mask(av[mb].x, P.tri_a, P.unit_a, ra + arow0, ks + k);
+              av[mb].y = tri_mask(av[mb].y, P.tri_a, P.unit_a, ra + arow1, ks + k);
+            }
+          }
+#pragma unroll
+          for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int nb8 = 0; nb8 < 4; ++nb8) {
+              double b;
+              if constexpr (LB == LAYOUT_R) {
+                const double2 v = bv[2 * (nb8 >> 1) + s2];
+                b = (nb8 & 1) ? v.y : v.x;
+              } else {
+                b = s2 ? bv[nb8].y : bv[nb8].x;
+              }
+              dmma_16x8x4(acc[mb][nb8], av[mb].x, av[mb].y, b);
+            }
+        }
+      } else {
 #pragma unroll
       for (int mb = 0; mb < 4; ++mb) {
         // A fragments of m16 block mb: av[s2] = (row arow0, row arow1) at step 2q + s2
@@ -332,21 +385,21 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
       }
     }
+      }
     }   // got
     // every warp is done with stage s: refill it with k block kt + STAGES
     if (!__syncthreads_and(got)) {
       ok = false;
       break;
     }
-    if (threadIdx.x == 0 && issued < KT) issue(issued++);
+    if (threadIdx.x == 0) produce();
   }
   if (!ok) {
     // a wait gave up: record it, and let thread 0 wait (bounded) for the copies it
     // issued before the CTA exits
     if (lane == 0) atomicExch(P.err, 3);
     if (threadIdx.x == 0)
-      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
-        mbar_wait(&full_bar[kt % STAGES], (kt / STAGES) & 1);
+      for (long long q = consumed; q < issued; ++q) mbar_wait(&full_bar[q % STAGES], (unsigned)((q / STAGES) & 1));
     return;
   }
 
@@ -407,6 +460,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
         }
   }
+  }   // tile loop
 }
 
 }  // namespace dmma

@@ -196,7 +196,10 @@ bool try_dmma(CULAPACKhandle h, const GemmProblem<double>& p, cudaStream_t s, co
               (p.cin == nullptr || (p.cin_rs == p.c_rs && p.cin_cs == p.c_cs) || p.cin != p.c);
   q.neg = q.preload && p.alpha == -1.0;
   q.err = h->d_words + 3;
-  const int tiles = ((p.m + dmma::BM - 1) / dmma::BM) * q.tiles_n;
+  q.tiles_m = (p.m + dmma::BM - 1) / dmma::BM;
+  const int all_tiles = q.tiles_m * q.tiles_n;
+  // one tile per CTA: several tiles per CTA measured slower (tails, uneven skipping)
+  const int tiles = all_tiles;
   const bool tri = p.tri_a || p.tri_b || p.unit_a || p.unit_b;
   *rc = tri ? launch_dmma_layouts<true>(h, la, lb, ma, mb, q, tiles, s, abort)
             : launch_dmma_layouts<false>(h, la, lb, ma, mb, q, tiles, s, abort);
@@ -284,22 +287,27 @@ CUresult set_smem(const void* fn, size_t bytes) {
 }
 
 // ---- ?POTRF ---------------------------------------------------------------------
-// Right-looking blocked Cholesky with lookahead depth 1, on two streams:
-//   panel stream : diagonal-block factor + inverse W (one CTA) -> panel solve
-//                  P = A21 W^H (tensor-core GEMM into the packed buffer P)
-//                  -> [wait previous trailing update] -> update of the next block
-//                  column (lookahead)
-//   update stream: [wait panel] -> copy P into A21 -> update of the rest of the
-//                  trailing matrix
-// so the next panel is factored on a few SMs while the previous trailing update
-// still runs on the rest.  P is a ping-pong pair of packed panel buffers.
-// Failure: the diagonal kernel sets the device info word, and every later kernel
-// exits at entry when it is set.
+// Right-looking blocked Cholesky, outer blocks of 2*nb columns (each factored as two
+// nb-wide sub-panels), lookahead depth 1, on two streams:
+//   panel stream : for each sub-panel: diagonal-block factor + inverse W (one CTA)
+//                  -> panel solve P = A21 W^H (tensor-core GEMM into the packed
+//                  buffer P); between the two sub-panels, the update of the second
+//                  one by the first.  Then [wait previous trailing update] -> update
+//                  of the next outer block (lookahead, k = 2*nb)
+//   update stream: [wait panel] -> copy P into A -> update of the rest of the
+//                  trailing matrix (k = 2*nb)
+// The next outer block is factored on a few SMs while the trailing update of the
+// previous one runs on the rest; the wide outer block halves the number of
+// trailing-update tiles per flop (their fill and drain are the engine's overhead).
+// P (ping-pong pair) holds rows from the first sub-panel's diagonal block down:
+// P(r, c) = L(j + nb + r, j + c).  Failure: the diagonal kernel sets the device
+// info word, and every later kernel exits at entry when it is set.
 constexpr int kDiagThreads2 = 256;
 
 template <typename T>
 CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out) {
   constexpr int nb = Tune<T>::nb;
+  constexpr int NB = 2 * nb;
   using Smem = DiagSmem<T, nb>;
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
   auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
@@ -307,10 +315,10 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   int* d_info = h->d_words;
 
   const long long ldp = (long long)round_up((size_t)n, 2);
-  const size_t ws = sizeof(T) * ((size_t)nb * nb + 2 * (size_t)ldp * nb);
+  const size_t ws = sizeof(T) * ((size_t)nb * nb + 2 * (size_t)ldp * NB);
   CUCHOL_CHECK_CU(ensure_workspace(h, ws));
   T* winv = static_cast<T*>(h->ws);
-  T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * nb};
+  T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * NB};
 
   CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_factor_kernel<T, nb, kDiagThreads2>, Smem::bytes));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
@@ -320,51 +328,60 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
   CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
 
-  for (int j = 0, step = 0; j < n; j += nb, ++step) {
-    const int jb = std::min(nb, n - j);
-    const int m = n - j - jb;
-    diag_factor_kernel<T, nb, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
-        at(j, j), rs, cs, jb, m > 0 ? winv : nullptr, nb, j, d_info, h->d_logdet);
-    ++h->launches;
-    CUCHOL_CHECK(cudaGetLastError());
-    if (m == 0) break;
-    T* P = pbuf[step & 1];
-
-    // panel solve: P = A21 * inv(L11)^H (W holds explicit zeros above its diagonal)
-    GemmProblem<T> t = problem<T>();
-    t.a = at(j + jb, j); t.a_rs = rs; t.a_ks = cs;
-    t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;
-    t.c = P; t.c_rs = 1; t.c_cs = ldp;
-    t.m = m; t.n = jb; t.k = jb;
-    CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
-    CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
-
-    // update stream: the solved panel into A, off the panel stream's critical path
-    CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
-    CUCHOL_CHECK_CU(copy_view<T>(h, P, 1, ldp, at(j + jb, j), rs, cs, m, jb, false, su, d_info));
-
-    // lookahead: next block column, after the previous trailing update
-    const int jb2 = std::min(nb, m);
-    CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+  const T minus_one = from_real<T>(RealOf<T>(-1)), one = from_real<T>(RealOf<T>(1));
+  // C -= Ahat Bhat^H on a lower-only view of A at (r0, c0), operands rows of P
+  auto update = [&](long long r0, long long c0, int m, int ncols, const T* pa, const T* pb, int k,
+                    cudaStream_t s) -> CUresult {
     GemmProblem<T> u = problem<T>();
-    u.a = P; u.a_rs = 1; u.a_ks = ldp;
-    u.b = P; u.b_rs = 1; u.b_ks = ldp; u.conj_b = 1;
-    u.c = at(j + jb, j + jb); u.c_rs = rs; u.c_cs = cs;
+    u.a = pa; u.a_rs = 1; u.a_ks = ldp;
+    u.b = pb; u.b_rs = 1; u.b_ks = ldp; u.conj_b = 1;
+    u.c = at(r0, c0); u.c_rs = rs; u.c_cs = cs;
     u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
-    u.alpha = from_real<T>(RealOf<T>(-1)); u.beta = from_real<T>(RealOf<T>(1));
+    u.alpha = minus_one; u.beta = one;
     u.lower_only = 1; u.real_diag = 1;
-    u.m = m; u.n = jb2; u.k = jb;
-    CUCHOL_CHECK_CU(gemm<T>(h, u, sp, d_info));
+    u.m = m; u.n = ncols; u.k = k;
+    return gemm<T>(h, u, s, d_info);
+  };
 
-    // rest of the trailing matrix
-    if (m > jb2) {
-      GemmProblem<T> r = u;
-      r.a = P + jb2; r.b = P + jb2;
-      r.c = at(j + jb + jb2, j + jb + jb2); r.cin = r.c;
-      r.m = m - jb2; r.n = m - jb2;
-      CUCHOL_CHECK_CU(gemm<T>(h, r, su, d_info));
+  for (int j = 0, step = 0; j < n; j += NB, ++step) {
+    const int jB = std::min(NB, n - j);
+    const int m = n - j - jB;                    // rows below the outer block
+    T* P = pbuf[step & 1];
+    for (int s0 = 0; s0 < jB; s0 += nb) {
+      const int c = j + s0, jb = std::min(nb, j + jB - c);
+      const int mr = n - c - jb;                 // rows below this diagonal block
+      diag_factor_kernel<T, nb, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
+          at(c, c), rs, cs, jb, mr > 0 ? winv : nullptr, nb, c, d_info, h->d_logdet);
+      ++h->launches;
+      CUCHOL_CHECK(cudaGetLastError());
+      if (mr == 0) break;
+      // panel solve into P: rows c + jb .. n-1 are P rows s0 .. (P starts at j + nb)
+      T* Ps = P + s0 + (long long)s0 * ldp;
+      GemmProblem<T> t = problem<T>();
+      t.a = at(c + jb, c); t.a_rs = rs; t.a_ks = cs;
+      t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;   // zeros above W's diagonal
+      t.c = Ps; t.c_rs = 1; t.c_cs = ldp;
+      t.m = mr; t.n = jb; t.k = jb;
+      CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
+      CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+      // update stream: the solved rows into A, off the panel stream's critical path
+      CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+      CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
+      if (s0 == 0 && jB > nb) {
+        // the second sub-panel's columns (rows j + nb ..) by the first sub-panel
+        CUCHOL_CHECK_CU(update(j + nb, j + nb, n - j - nb, jB - nb, P, P, nb, sp));
+      }
     }
-    // always recorded: it also covers the copy that still reads P
+    if (m == 0) break;
+    // lookahead: next outer block (P rows from j + NB, k = jB), after the previous
+    // trailing update
+    const int jB2 = std::min(NB, m);
+    const T* Pt = P + nb;
+    CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+    CUCHOL_CHECK_CU(update(j + NB, j + NB, m, jB2, Pt, Pt, jB, sp));
+    // rest of the trailing matrix
+    if (m > jB2) CUCHOL_CHECK_CU(update(j + NB + jB2, j + NB + jB2, m - jB2, m - jB2, Pt + jB2, Pt + jB2, jB, su));
+    // always recorded: it also covers the copies that still read P
     CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   }
   CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
