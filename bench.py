@@ -50,7 +50,31 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--syrk", nargs=2, type=int, metavar=("M", "K"),
+                    help="only the dominant kernel: two cuDsyrk(L, N) launches of order M, rank K "
+                         "(warm-up + measured), for profiling")
     return ap.parse_args()
+
+
+def run_syrk_only(m: int, k: int) -> None:
+    import torch
+    import cucholesky as cc
+    dev = torch.device("cuda", 0)
+    bh = cc.BlasHandle()
+    P = torch.randn(k, m, dtype=torch.float64, device=dev)     # column-major m x k
+    C = torch.zeros(m, m, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream()
+    for _ in range(2):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc = cc.call_rankk(bh, "D", "L", "N", m, k, -1.0, P.data_ptr(), m, 1.0, C.data_ptr(), m, st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(json.dumps({"kernel": "cuDsyrk L,N", "m": m, "k": k, "rc": rc, "ms": ms,
+                          "tflops": float(m) * (m + 1) * k / (ms / 1e3) / 1e12}), flush=True)
+    bh.close()
 
 
 def dist_env():
@@ -201,6 +225,9 @@ def make_spd_device(torch, n, seed, dev):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.syrk:
+        run_syrk_only(*args.syrk)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return
@@ -263,6 +290,32 @@ def main():
         if pg:
             pg.barrier()
     nlaunch = launches() - l0
+
+    # the dominant kernel alone: the trailing update (tensor-core SYRK) at the shape
+    # of the factorization's first outer step, m = n - 512 rows, k = 256, timed with
+    # CUDA events on the stream it is launched on
+    bh = cc.BlasHandle()
+    mk, kk = n - 512, 256
+    Pk = torch.randn(kk, mk, dtype=torch.float64, device=dev)     # column-major mk x kk
+    Ck = torch.zeros(mk, mk, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream()
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(3)]
+    cc.call_rankk(bh, "D", "L", "N", mk, kk, -1.0, Pk.data_ptr(), mk, 1.0, Ck.data_ptr(), mk, st.cuda_stream)
+    for a, b in kev:
+        a.record(st)
+        rc = cc.call_rankk(bh, "D", "L", "N", mk, kk, -1.0, Pk.data_ptr(), mk, 1.0, Ck.data_ptr(), mk,
+                           st.cuda_stream)
+        b.record(st)
+    torch.cuda.synchronize()
+    syrk_ms = statistics.mean(a.elapsed_time(b) for a, b in kev)
+    syrk_flops = float(mk) * (mk + 1) * kk          # lower triangle incl. diagonal
+    syrk_tflops = syrk_flops / (syrk_ms / 1e3) / 1e12
+    # DRAM traffic per launch: 15.1 bytes per lower-triangle element of C, from the
+    # ncu capture of the same kernel at m = 8192, k = 256 (profiles/), scaled by the
+    # number of C elements (C's read + write dominate; the panel stays in L2)
+    syrk_traffic = 15.1 * (float(mk) * (mk + 1) / 2)
+    del Pk, Ck
+    bh.close()
     total_ms = t0.elapsed_time(t1)
     potrf_ms = [a.elapsed_time(b) for a, b in evs]
     if pg:
@@ -329,9 +382,14 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single"},
             "potrf_ms": statistics.mean(potrf_ms),
             "backward_error_sampled": berr,
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+            "roofline": {"bound": "tensor", "achieved": syrk_tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": syrk_tflops / peak, "traffic": syrk_traffic,
+                         "kernel": f"dmma::gemm_kernel<0,0,0>: trailing-update SYRK (cuDsyrk L,N) m={mk} k={kk}",
+                         "kernel_ms": syrk_ms, "algorithmic_flop": syrk_flops,
+                         "algorithmic_bytes": 16.0 * (float(mk) * (mk + 1) / 2) + 8.0 * mk * kk,
                          "peak_source": "FP64 dense peak measured live: best cuBLAS DGEMM 8192^3 on this GPU"},
+            "potrf_fraction_of_peak": achieved / peak,
+            "potrf_achieved_tflops": achieved,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": nlaunch,
