@@ -31,6 +31,7 @@ struct GemmProblem {
   uint8_t unit_a, unit_b;   // a triangular view has an implicit unit diagonal
   uint8_t lower_only;   // write only i >= j; tiles wholly above the diagonal exit
   uint8_t real_diag;    // store Im C(i, i) = 0 (Hermitian results)
+  const int* stop;      // grouped launches: skip the problem when this word is set
   int tiles_n;          // tile columns of this problem (filled by the launcher)
   int tile_begin;       // first tile index of this problem in a grouped launch
 };
@@ -84,6 +85,7 @@ gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict_
   if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
 
   const GemmProblem<T>& P = *find_problem(L, blockIdx.x);
+  if (P.stop != nullptr && *(volatile const int*)P.stop != 0) return;
   const int tile = blockIdx.x - P.tile_begin;
   const int ti = tile / P.tiles_n, tj = tile % P.tiles_n;
   const int i0 = ti * BM, j0 = tj * BN;

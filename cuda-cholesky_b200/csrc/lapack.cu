@@ -919,3 +919,5 @@ CUCHOL_API_RANKK(cuSsyrk, float, false)
 CUCHOL_API_RANKK(cuDsyrk, double, false)
 CUCHOL_API_RANKK(cuCherk, cuFloatComplex, true)
 CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
+
+#include "batched.cuh"

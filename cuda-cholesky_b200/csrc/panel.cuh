@@ -288,9 +288,9 @@ __device__ void assemble_inverse(T* S, int LD, int jb, const T* X, T* TMP, int t
 // On failure at local column k: *d_info = info_base + k + 1 (if still 0), the
 // partially factored block is written back, W is not written.
 template <typename T, int NB, int NT>
-__global__ void __launch_bounds__(NT)
-diag_factor_kernel(T* __restrict__ A, long long rs, long long cs, int jb, T* __restrict__ W, int ldw,
-                   long long info_base, int* __restrict__ d_info, double* __restrict__ logdet) {
+__device__ __forceinline__ void diag_factor_block(T* __restrict__ A, long long rs, long long cs, int jb,
+                                                  T* __restrict__ W, int ldw, long long info_base,
+                                                  int* __restrict__ d_info, double* __restrict__ logdet) {
   using R = RealOf<T>;
   using L = DiagSmem<T, NB>;
   constexpr int LD = L::LD;
@@ -368,7 +368,61 @@ diag_factor_kernel(T* __restrict__ A, long long rs, long long cs, int jb, T* __r
 // written; unit: the diagonal is taken as 1 and left untouched.
 template <typename T, int NB, int NT>
 __global__ void __launch_bounds__(NT)
+diag_factor_kernel(T* __restrict__ A, long long rs, long long cs, int jb, T* __restrict__ W, int ldw,
+                   long long info_base, int* __restrict__ d_info, double* __restrict__ logdet) {
+  diag_factor_block<T, NB, NT>(A, rs, cs, jb, W, ldw, info_base, d_info, logdet);
+}
+
+// One diagonal block of one matrix of a batch (batched factor: one CTA per task).
+template <typename T>
+struct DiagTask {
+  T* a;               // top-left of the block, logical lower view (strides rs, cs)
+  long long rs, cs;
+  int jb;
+  T* w;               // inverse of the factored block (ld ldw), or null
+  int ldw;
+  long long info_base;
+  int* info;          // the matrix's info word (later steps skip once it is set)
+  double* logdet;     // the matrix's log det accumulator, or null
+};
+
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT) diag_factor_batched_kernel(const DiagTask<T>* __restrict__ tasks) {
+  const DiagTask<T> t = tasks[blockIdx.x];
+  diag_factor_block<T, NB, NT>(t.a, t.rs, t.cs, t.jb, t.w, t.ldw, t.info_base, t.info, t.logdet);
+}
+
+template <typename T, int NB, int NT>
+__device__ __forceinline__ void diag_invert_block(T* __restrict__ B, long long rs, long long cs, int jb,
+                                                  int unit);
+
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT)
 diag_invert_kernel(T* __restrict__ A, long long rs, long long cs, int n, int nb, int unit) {
+  const int o = blockIdx.x * nb;
+  diag_invert_block<T, NB, NT>(A + o * rs + o * cs, rs, cs, min(nb, n - o), unit);
+}
+
+// In-place inverse of one diagonal block of one matrix of a batch.
+template <typename T>
+struct InvTask {
+  T* b;               // top-left of the block (strides rs, cs)
+  long long rs, cs;
+  int jb;
+  int unit;
+  const int* stop;    // skip when this word is non-zero (the matrix's factor failed)
+};
+
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT) diag_invert_batched_kernel(const InvTask<T>* __restrict__ tasks) {
+  const InvTask<T> t = tasks[blockIdx.x];
+  if (t.stop != nullptr && *(volatile const int*)t.stop != 0) return;
+  diag_invert_block<T, NB, NT>(t.b, t.rs, t.cs, t.jb, t.unit);
+}
+
+template <typename T, int NB, int NT>
+__device__ __forceinline__ void diag_invert_block(T* __restrict__ B, long long rs, long long cs, int jb,
+                                                  int unit) {
   using R = RealOf<T>;
   using L = DiagSmem<T, NB>;
   constexpr int LD = L::LD;
@@ -377,9 +431,6 @@ diag_invert_kernel(T* __restrict__ A, long long rs, long long cs, int n, int nb,
   T* X = reinterpret_cast<T*>(smem_raw + L::S);
   T* TMP = reinterpret_cast<T*>(smem_raw + L::S + L::X);
   T* rdiag = reinterpret_cast<T*>(smem_raw + L::S + L::X + L::TMP);
-  const int o = blockIdx.x * nb;
-  const int jb = min(nb, n - o);
-  T* B = A + o * rs + o * cs;
   const bool rows_fast = (rs == 1);
   for (int e = threadIdx.x; e < jb * jb; e += NT) {
     int r, c;

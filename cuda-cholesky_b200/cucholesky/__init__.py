@@ -288,3 +288,82 @@ def call_rankk(bh: BlasHandle, p: str, uplo: str, trans: str, n: int, k: int, al
     name = {"S": "cuSsyrk", "D": "cuDsyrk", "C": "cuCherk", "Z": "cuZherk"}[p]
     return getattr(lib(), name)(bh.value, ord(uplo), ord(trans), n, k, _REAL[p](alpha), a, lda, _REAL[p](beta),
                                 c, ldc, C.c_void_p(stream))
+
+
+# ---- batched plan (include/cucholesky_ext.h) -------------------------------------
+
+BATCHED_POTRF, BATCHED_LOGDET, BATCHED_POTRI = 1, 2, 4
+
+
+class BatchedPlan:
+    """cu?cholBatchedCreate / Run / Results / Destroy for matrices packed in one
+    device buffer: matrix b is column-major n[b] x n[b] with leading dimension
+    lda[b], starting at element offset off[b] of `buf` (a torch tensor)."""
+
+    def __init__(self, h: Handle, buf, n, off, lda=None, uplo="L", flags=7, nb=0):
+        L = lib()
+        p = "D" if str(buf.dtype) == "torch.float64" else "S"
+        esize = buf.element_size()
+        self.batch = len(n)
+        lda = list(n) if lda is None else list(lda)
+        self._n = (C.c_int * self.batch)(*n)
+        self._lda = (C.c_int * self.batch)(*lda)
+        base = buf.data_ptr()
+        self._ptrs = (C.c_uint64 * self.batch)(*[base + int(o) * esize for o in off])
+        self._p = C.c_void_p()
+        f = getattr(L, f"cu{p}cholBatchedCreate")
+        f.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                      C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.c_int, C.c_int]
+        f.restype = C.c_int
+        rc = f(C.byref(self._p), h.value, ord(uplo), self.batch, self._n, self._ptrs, self._lda, flags, nb)
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError(f"cu{p}cholBatchedCreate", rc)
+        L.cuCholBatchedRun.argtypes = [C.c_void_p, C.c_void_p]
+        L.cuCholBatchedResults.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_double)]
+        L.cuCholBatchedGetBlockSize.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        L.cuCholBatchedDestroy.argtypes = [C.c_void_p]
+
+    @property
+    def nb(self) -> int:
+        v = C.c_int(0)
+        lib().cuCholBatchedGetBlockSize(self._p, C.byref(v))
+        return v.value
+
+    def run(self, stream: int = 0) -> None:
+        rc = lib().cuCholBatchedRun(self._p, C.c_void_p(stream))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuCholBatchedRun", rc)
+
+    def results(self):
+        info = (C.c_long * self.batch)()
+        ld = (C.c_double * self.batch)()
+        rc = lib().cuCholBatchedResults(self._p, info, ld)
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuCholBatchedResults", rc)
+        return list(info), list(ld)
+
+    def close(self):
+        if self._p:
+            lib().cuCholBatchedDestroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pack_colmajor(mats, dtype):
+    """Pack square column-major numpy matrices into one 1-D array; returns
+    (array, offsets, sizes)."""
+    import numpy as np
+    sizes = [m.shape[1] for m in mats]
+    off, t = [], 0
+    for m in mats:
+        off.append(t)
+        t += m.shape[0] * m.shape[1]
+    out = np.zeros(max(t, 1), dtype=dtype)
+    for m, o in zip(mats, off):
+        out[o:o + m.size] = np.asarray(m, dtype=dtype).ravel(order="F")
+    return out, off, sizes

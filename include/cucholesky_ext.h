@@ -24,6 +24,34 @@ CUresult cuCpotrfLogdet(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, 
  * measurement; counts this library's own kernels only). */
 CUresult cuLAPACKGetLaunchCount(CULAPACKhandle, unsigned long long *);
 
+/* Batched factor, log det and inverse of many small SPD matrices of uneven sizes
+ * (each matrix b: order n[b], device pointer A[b], leading dimension lda[b], all
+ * in the same `uplo` storage).  No counterpart in the reference library.
+ *
+ * A plan records the whole sequence once into a CUDA graph: all matrices advance
+ * one nb-wide block column per step, and each step is a few grouped launches over
+ * the batch (diagonal blocks, panel solves, trailing updates), followed, with
+ * CUCHOL_BATCHED_POTRI, by the grouped inverse.  nb = 0 lets the plan pick the
+ * block size by timing the candidates (32, 64) on an identity batch of the same
+ * shapes; otherwise nb must be 8..64 and a multiple of 8.  The plan keeps the
+ * pointers: run it again after refilling the same buffers.
+ *   cu?cholBatchedCreate  build (and tune) the plan; allocates its workspace
+ *   cuCholBatchedRun      one graph launch on `stream`
+ *   cuCholBatchedResults  waits, then copies info[b] (as ?potrf / ?potri) and
+ *                         log det A_b (with CUCHOL_BATCHED_LOGDET) to the host */
+typedef struct __cucholbatched_st * CUcholBatched;
+#define CUCHOL_BATCHED_POTRF  1
+#define CUCHOL_BATCHED_LOGDET 2
+#define CUCHOL_BATCHED_POTRI  4
+CUresult cuDcholBatchedCreate(CUcholBatched *, CULAPACKhandle, CBlasUplo, int, const int *, const CUdeviceptr *,
+                              const int *, int, int);
+CUresult cuScholBatchedCreate(CUcholBatched *, CULAPACKhandle, CBlasUplo, int, const int *, const CUdeviceptr *,
+                              const int *, int, int);
+CUresult cuCholBatchedRun(CUcholBatched, CUstream);
+CUresult cuCholBatchedResults(CUcholBatched, long *, double *);
+CUresult cuCholBatchedGetBlockSize(CUcholBatched, int *);
+CUresult cuCholBatchedDestroy(CUcholBatched);
+
 /* log det from a strided FP64 diagonal, 2 * sum_i log(x[i*incx]), for callers that
  * cannot allocate device memory.  No counterpart in the reference library.
  *
