@@ -50,7 +50,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="potrf", choices=["potrf", "batched"],
+    ap.add_argument("--kappa", default="0,1,2,3",
+                    help="mixed workload: exponents k of D = diag(10^(k i/(n-1))), comma separated")
+    ap.add_argument("--workload", default="potrf", choices=["potrf", "batched", "mixed"],
                     help="potrf: FP64 dpotrf n=16384 (default line); batched: 10,000 uneven SPD "
                          "kernel matrices, potrf + logdet + potri in one graph launch")
     ap.add_argument("--dtype", default="d", choices=["d", "s"], help="batched workload precision")
@@ -328,6 +330,109 @@ def run_batched(args) -> None:
     h.close()
 
 
+def run_mixed(args) -> None:
+    """Mixed-precision refined SPD solve against the plain FP64 solve on the same GPU,
+    n = 32768, 16 right-hand sides ~ N(0, 1): A = D (G G^T / n + 1e-3 I) D with
+    G ~ N(0, 1) and D = diag(10^(k i / (n - 1))) for each k of --kappa (kappa ~1e3 to
+    ~1e9).  FP64 arm: cuDpotrf + cuDpotrs on a restored copy of A.  Mixed arm, BF16
+    and TF32 trailing updates: cuDcholMixedRefactor (scaling, |A|_inf, low-precision
+    factor) + cuDcholMixedSolve (FP64 refinement to sqrt(n) eps).  Backward errors
+    are recomputed here in FP64 (torch) for both arms."""
+    import torch
+    import cucholesky as cc
+    from cucholesky import matgen
+    dev = torch.device("cuda", 0)
+    n = args.n if args.n != N_DEFAULT else 32768
+    nrhs = 16
+    ks = [float(k) for k in args.kappa.split(",")]
+    h = cc.Handle()
+    cases = []
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for k in ks:
+        A = matgen.scaled_spd_device(n, k, seed=int(k), device=dev)
+        g = torch.Generator(device=dev)
+        g.manual_seed(100 + int(k))
+        B = torch.randn((nrhs, n), generator=g, device=dev, dtype=torch.float64)   # column-major n x 16
+        anorm = A.abs().sum(dim=1).max().item()
+
+        def berr(X):
+            R = B - X @ A
+            return float(max(R[c].abs().max().item() / (anorm * X[c].abs().max().item() + B[c].abs().max().item())
+                             for c in range(nrhs)))
+
+        # FP64: dpotrf + dpotrs
+        Aw = torch.empty_like(A)
+        X64 = torch.empty_like(B)
+        t64 = []
+        for it in range(args.warmup + args.steps):
+            Aw.copy_(A)
+            X64.copy_(B)
+
+            def fp64():
+                rc, info = cc.call_potrf(h, "D", "L", n, Aw.data_ptr(), n)
+                assert rc == 0 and info == 0, (rc, info)
+                rc, info = cc.call_potrs(h, "D", "L", n, nrhs, Aw.data_ptr(), n, X64.data_ptr(), n)
+                assert rc == 0 and info == 0
+            ms, _ = timed(fp64)
+            if it >= args.warmup:
+                t64.append(ms)
+        b64 = berr(X64)
+        del Aw
+        torch.cuda.empty_cache()
+        for prec, pname in ((cc.MIXED_TF32, "tf32"), (cc.MIXED_BF16, "bf16")):
+            X = torch.zeros_like(B)
+            plan = cc.MixedPlan(h, "L", n, A.data_ptr(), n, prec)
+            tf, ts, iters = [], [], []
+            res = (0, 0.0)
+            for it in range(args.warmup + args.steps):
+                msf, info = timed(plan.refactor)
+                assert info == 0, info
+                mss, res = timed(lambda: plan.solve(nrhs, B.data_ptr(), n, X.data_ptr(), n))
+                if it >= args.warmup:
+                    tf.append(msf)
+                    ts.append(mss)
+                    iters.append(res[0])
+            shift = plan.factor()[4]
+            plan.close()
+            bm = berr(X)
+            fwd = float((X - X64).abs().max().item() / X64.abs().max().item())
+            t_mixed = statistics.mean(tf) + statistics.mean(ts)
+            cases.append({
+                "k": k, "precision": pname, "fp64_ms": statistics.mean(t64), "mixed_ms": t_mixed,
+                "factor_ms": statistics.mean(tf), "refine_ms": statistics.mean(ts), "iterations": iters[-1],
+                "speedup": statistics.mean(t64) / t_mixed, "berr_mixed": bm, "berr_fp64": b64,
+                "berr_bound_10_n_eps": 10 * n * 2.0 ** -52, "rel_diff_vs_fp64_solution": fwd, "shift": shift,
+                "effective_fp64_tflops_factor": n ** 3 / 3 / (statistics.mean(tf) / 1e3) / 1e12,
+            })
+            del X
+        del A, B
+        torch.cuda.empty_cache()
+    ok = [c for c in cases if c["k"] <= 2.0 and c["precision"] == "tf32"]
+    value = min(c["speedup"] for c in ok) if ok else None
+    line = {
+        "metric": "mixed_refined_solve_speedup_vs_fp64_dpotrf_dpotrs", "value": value, "unit": "x",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": min(c["mixed_ms"] for c in ok) if ok else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (tf32/bf16 trailing updates)", "data": "synthetic",
+        "config": {"workload": "SPD solve A = D (G G^T/n + 1e-3 I) D, G ~ N(0,1), D = diag(10^(k i/(n-1))), "
+                               "16 rhs ~ N(0,1), lower", "n": n, "nrhs": nrhs, "k": ks,
+                   "value": "min over k <= 2 (kappa <= ~4e7) of the TF32 speedup"},
+        "cases": cases,
+    }
+    print(json.dumps(line), flush=True)
+    h.close()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -337,6 +442,10 @@ def main():
     if args.workload == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.workload == "mixed":
+        if rank == 0:
+            run_mixed(args)
         return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)

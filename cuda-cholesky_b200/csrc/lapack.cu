@@ -921,3 +921,4 @@ CUCHOL_API_RANKK(cuCherk, cuFloatComplex, true)
 CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 
 #include "batched.cuh"
+#include "mixed.cuh"

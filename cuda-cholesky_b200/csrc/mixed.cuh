@@ -1,0 +1,1233 @@
+// Mixed-precision SPD solve and the FP64 triangular solves under it (included at
+// the end of lapack.cu; uses its launch helpers).  No counterpart in the reference
+// library, which stops at ?potrf / ?potri (lapack/dpotrf.c:172, lapack/dpotri.c:25):
+// the solve follows LAPACK's DSPOSV contract (low-precision factor, FP64
+// refinement, FP64 fallback) on the dense SPD path of this library.
+//
+// Factor (cuDcholMixedCreate):
+//   1. s_i = 1 / sqrt(a_ii); W = S A S + shift * I in FP32 (lower, our own buffer):
+//      the symmetric diagonal scaling removes the row/column scaling part of
+//      kappa(A) before any rounding to low precision.
+//   2. Right-looking blocked Cholesky of W with the same two-stream schedule as
+//      ?potrf (outer blocks of 256 columns = two 128-column sub-panels, lookahead):
+//        - diagonal blocks in FP64 (the ?potrf diagonal kernel on an FP64 copy),
+//        - panel solve P = W21 inv(L11)^T in FP32 (SIMT engine) into a k-major
+//          buffer, then copied into W and rounded to the operand type Q (BF16 or
+//          TF32),
+//        - trailing updates W22 -= Q Q^T on the tcgen05 tensor cores with FP32
+//          accumulation (tc.cuh).
+//   3. The inverses of W's 64 x 64 diagonal blocks (for the triangular solves).
+// Solve (cuDcholMixedSolve): preconditioned conjugate gradients in FP64 on A x = b
+// with M^-1 = S L^-T L^-1 S, in groups of 16 right-hand sides, as iterative
+// refinement: the loop ends when every normwise backward error
+//   |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf)
+// computed from a freshly formed FP64 residual is below the tolerance.
+// A x uses the FP64 A in the caller's storage (symmetric product from one
+// triangle, deterministic); the triangular solves are single launches in which
+// row blocks are taken in ticket order and wait (bounded) for the blocks they
+// depend on.
+
+#include "tc.cuh"
+
+namespace {
+namespace mx {
+
+constexpr int SB = 128;        // sub-panel width: FP64 diagonal blocks
+constexpr int OB = 2 * SB;     // outer block
+constexpr int BS = 64;         // triangular-solve block
+constexpr int NR = 16;         // right-hand sides per group
+constexpr int SY = 256;        // symmetric-product tile
+constexpr int kThreads = 256;
+
+// ---- factor kernels --------------------------------------------------------------
+
+// s_i = 1 / sqrt(A(i, i)); a diagonal that is not positive sets *bad.
+__global__ void scale_kernel(const double* __restrict__ A, long long dstride, int n, double* __restrict__ s,
+                             int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = A[(long long)i * dstride];
+  if (!(a > 0.0)) atomicExch(bad, 1);
+  s[i] = (a > 0.0) ? 1.0 / sqrt(a) : 0.0;
+}
+
+// W(i, j) = s_i A(i, j) s_j (+ shift on the diagonal) for i >= j, FP32.  A is the
+// logical lower view A(i, j) = a[i*rs + j*cs]; 32 x 32 tiles through shared memory
+// so that both the read (either storage) and the write are coalesced.
+__global__ void build_kernel(const double* __restrict__ a, long long rs, long long cs, int n,
+                             const double* __restrict__ s, float shift, float* __restrict__ W, long long ldw) {
+  __shared__ double t[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  if (j0 > i0 + 31) return;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+  const bool row_contig = (rs == 1);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = ty + 8 * k;
+    // element (ii, jj) of the tile read by this thread
+    const int ii = row_contig ? tx : r, jj = row_contig ? r : tx;
+    const int i = i0 + ii, j = j0 + jj;
+    t[ii][jj] = (i < n && j < n && i >= j) ? a[(long long)i * rs + (long long)j * cs] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int jj = ty + 8 * k, i = i0 + tx, j = j0 + jj;
+    if (i < n && j < n && i >= j) {
+      float w = (float)(s[i] * t[tx][jj] * s[j]);
+      if (i == j) w += shift;
+      W[i + (long long)j * ldw] = w;
+    }
+  }
+}
+
+// FP32 diagonal block of W -> FP64 copy D (ld SB); column j = blockIdx.x.
+__global__ void diag_in_kernel(const float* __restrict__ W, long long ldw, int jb, double* __restrict__ D,
+                               const int* __restrict__ stop) {
+  if (*stop != 0) return;
+  const int j = blockIdx.x, i = threadIdx.x;
+  if (i < jb && i >= j) D[i + j * SB] = (double)W[i + (long long)j * ldw];
+}
+
+// Factored FP64 block -> W (FP32), and the FP64 inverse -> FP32 (ld SB).
+__global__ void diag_out_kernel(const double* __restrict__ D, const double* __restrict__ winv, int jb,
+                                float* __restrict__ W, long long ldw, float* __restrict__ winv32,
+                                const int* __restrict__ stop) {
+  if (*stop != 0) return;
+  const int j = blockIdx.x, i = threadIdx.x;
+  if (i >= jb) return;
+  if (i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
+  if (winv != nullptr) winv32[i + j * SB] = (float)winv[i + j * SB];
+}
+
+__device__ __forceinline__ float round_tf32(float x) {
+  uint32_t u;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+  return __uint_as_float(u);
+}
+template <typename Op> __device__ __forceinline__ Op to_op(float x);
+template <> __device__ __forceinline__ __nv_bfloat16 to_op<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+template <> __device__ __forceinline__ float to_op<float>(float x) { return round_tf32(x); }
+
+// Solved panel rows (k-major FP32 P, row pitch ldq) -> W (column-major) and the
+// tensor-core operand Q (k-major, rounded to BF16 or TF32).  32 x 32 tiles.
+template <typename Op>
+__global__ void panel_store_kernel(const float* __restrict__ P, long long ldq, int mr, int jb,
+                                   float* __restrict__ W, long long ldw, Op* __restrict__ Q,
+                                   const int* __restrict__ stop) {
+  if (*stop != 0) return;
+  __shared__ float t[32][33];
+  const int r0 = blockIdx.x * 32, q0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = r0 + ty + 8 * k, q = q0 + tx;
+    float v = 0.f;
+    if (r < mr && q < jb) {
+      v = P[(long long)r * ldq + q];
+      Q[(long long)r * ldq + q] = to_op<Op>(v);
+    }
+    t[ty + 8 * k][tx] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int q = q0 + ty + 8 * k, r = r0 + tx;
+    if (r < mr && q < jb) W[r + (long long)q * ldw] = t[tx][ty + 8 * k];
+  }
+}
+
+// ---- triangular solves ------------------------------------------------------------
+
+// Inverse of the 64 x 64 diagonal blocks of a lower-triangular L (logical view
+// L(i, j) = L[i*rs + j*cs]); DI[b] is column-major 64 x 64 with zeros above the
+// diagonal.  Rows past n of the last block are given a unit diagonal.  One CTA per
+// block, one thread per column of the inverse (forward substitution).
+template <typename T>
+__global__ void __launch_bounds__(BS) block_inverse_kernel(const T* __restrict__ L, long long rs, long long cs,
+                                                           int n, T* __restrict__ DI) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);   // [BS][BS + 1], row-major
+  T* X = Ls + BS * (BS + 1);                // [BS][BS + 1]
+  const int b = blockIdx.x, i0 = b * BS, t = threadIdx.x;
+  const bool row_contig = (rs == 1);
+  for (int e = t; e < BS * BS; e += BS) {
+    const int i = row_contig ? (e % BS) : (e / BS), j = row_contig ? (e / BS) : (e % BS);
+    T v = T(0);
+    if (i0 + i < n && i >= j) v = L[(long long)(i0 + i) * rs + (long long)(i0 + j) * cs];
+    if (i0 + i >= n && i == j) v = T(1);
+    Ls[i * (BS + 1) + j] = v;
+  }
+  __syncthreads();
+  const int c = t;   // column of the inverse
+  for (int i = 0; i < BS; ++i) {
+    T x = T(0);
+    if (i >= c) {
+      T acc = (i == c) ? T(1) : T(0);
+      for (int k = c; k < i; ++k) acc -= Ls[i * (BS + 1) + k] * X[k * (BS + 1) + c];
+      x = acc / Ls[i * (BS + 1) + i];
+    }
+    X[i * (BS + 1) + c] = x;
+  }
+  __syncthreads();
+  T* out = DI + (size_t)b * BS * BS;
+  for (int e = t; e < BS * BS; e += BS) out[e] = X[(e % BS) * (BS + 1) + e / BS];
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0 waits until *ready >= need (bounded); returns the value seen.  A wait
+// that gives up sets *err and returns `need`, so that the solve still ends.
+__device__ __forceinline__ unsigned wait_ready(const unsigned* ready, unsigned need, int* err) {
+  for (unsigned it = 0; it < (1u << 24); ++it) {
+    const unsigned v = ld_acquire(ready);
+    if (v >= need) return v;
+    if (it > 64) __nanosleep(64);
+  }
+  atomicExch(err, 1);
+  return need;
+}
+
+// Y := L^-1 (sc .* B) for up to NR right-hand sides; L lower (view strides rs, cs),
+// B of type VB (ldb), Y of type T (ldy, at least 64 * ceil(n / 64) rows).  One CTA
+// per 64-row block, blocks taken in ticket order; block I accumulates L(I, J) y_J
+// for J < I as the y_J are published (the counter ready = number of finished
+// blocks), then applies DI_I.
+// Counters: ctr[0] ticket, ctr[1] ready; both zero at launch.
+template <typename T, typename VB>
+__global__ void __launch_bounds__(kThreads)
+    trsv_fwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
+                    const VB* __restrict__ B, long long ldb, const double* __restrict__ sc, T* Y, long long ldy,
+                    int nrhs, unsigned* ctr, int* err) {
+  __shared__ T Ls[BS][BS + 1];
+  __shared__ T Vs[BS][NR];
+  __shared__ unsigned s_I, s_known;
+  const int t = threadIdx.x, r = t & (BS - 1), g = t >> 6;
+  if (t == 0) {
+    s_I = atomicAdd(&ctr[0], 1u);
+    s_known = 0;
+  }
+  __syncthreads();
+  const int I = (int)s_I, i0 = I * BS, i = i0 + r;
+  const bool row_contig = (rs == 1);
+  T acc[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c = g * 4 + k;
+    acc[k] = (i < n && c < nrhs) ? (T)(sc != nullptr ? sc[i] * (double)B[i + c * ldb] : (double)B[i + c * ldb])
+                                 : T(0);
+  }
+  // prefetch of the next L block: element e = t + 256 q
+  T pre[BS * BS / kThreads];
+  auto fetch = [&](int J) {
+#pragma unroll
+    for (int q = 0; q < BS * BS / kThreads; ++q) {
+      const int e = t + kThreads * q;
+      const int ii = row_contig ? (e % BS) : (e / BS), jj = row_contig ? (e / BS) : (e % BS);
+      pre[q] = (i0 + ii < n) ? L[(long long)(i0 + ii) * rs + (long long)(J * BS + jj) * cs] : T(0);
+    }
+  };
+  if (I > 0) fetch(0);
+  for (int J = 0; J < I; ++J) {
+#pragma unroll
+    for (int q = 0; q < BS * BS / kThreads; ++q) {
+      const int e = t + kThreads * q;
+      const int ii = row_contig ? (e % BS) : (e / BS), jj = row_contig ? (e / BS) : (e % BS);
+      Ls[ii][jj] = pre[q];
+    }
+    if (J + 1 < I) fetch(J + 1);
+    if (t == 0 && s_known < (unsigned)(J + 1)) s_known = wait_ready(&ctr[1], (unsigned)(J + 1), err);
+    __syncthreads();
+    {
+      const int jj = t >> 4, c = t & 15;   // y_J into shared memory (L2 reads: written by another CTA)
+      Vs[jj][c] = __ldcg(&Y[(long long)(J * BS + jj) + c * ldy]);
+      const int jj2 = jj + 16;
+      Vs[jj2][c] = __ldcg(&Y[(long long)(J * BS + jj2) + c * ldy]);
+      Vs[jj2 + 16][c] = __ldcg(&Y[(long long)(J * BS + jj2 + 16) + c * ldy]);
+      Vs[jj2 + 32][c] = __ldcg(&Y[(long long)(J * BS + jj2 + 32) + c * ldy]);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int cc = 0; cc < BS; ++cc) {
+      const T l = Ls[r][cc];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] -= l * Vs[cc][g * 4 + k];
+    }
+    __syncthreads();
+  }
+  // y_I = DI_I acc
+#pragma unroll
+  for (int k = 0; k < 4; ++k) Vs[r][g * 4 + k] = acc[k];
+  __syncthreads();
+  const T* D = DI + (size_t)I * BS * BS;
+  T y[4] = {T(0), T(0), T(0), T(0)};
+  for (int cc = 0; cc <= r; ++cc) {
+    const T d = D[r + cc * BS];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) y[k] += d * Vs[cc][g * 4 + k];
+  }
+  if (i < n) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) __stcg(&Y[i + (long long)(g * 4 + k) * ldy], y[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) __stcg(&Y[i + (long long)(g * 4 + k) * ldy], T(0));
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) st_release(&ctr[1], (unsigned)(I + 1));
+}
+
+// Z := sc .* (L^-T Y) (type VZ, ldz), the transposed solve of trsv_fwd_kernel:
+// blocks taken from the last one; block I accumulates L(J, I)^T z_J for J > I.
+// ctr[1] counts finished blocks from the end.  Y and Z may alias (in place).
+template <typename T, typename VZ>
+__global__ void __launch_bounds__(kThreads)
+    trsv_bwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
+                    const T* Y, long long ldy, const double* __restrict__ sc, VZ* Z, long long ldz, T* Zt,
+                    int nrhs, unsigned* ctr, int* err) {
+  __shared__ T Ls[BS][BS + 1];   // Ls[c][r] = L(J*BS + c, I*BS + r)
+  __shared__ T Vs[BS][NR];
+  __shared__ unsigned s_I, s_known;
+  const int nblk = (n + BS - 1) / BS;
+  const int t = threadIdx.x, r = t & (BS - 1), g = t >> 6;
+  if (t == 0) {
+    s_I = atomicAdd(&ctr[0], 1u);
+    s_known = 0;
+  }
+  __syncthreads();
+  const int I = nblk - 1 - (int)s_I, i0 = I * BS, i = i0 + r;
+  const bool row_contig = (rs == 1);
+  T acc[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) acc[k] = (i < n) ? Y[i + (long long)(g * 4 + k) * ldy] : T(0);
+  T pre[BS * BS / kThreads];
+  auto fetch = [&](int J) {
+#pragma unroll
+    for (int q = 0; q < BS * BS / kThreads; ++q) {
+      const int e = t + kThreads * q;
+      const int cc = row_contig ? (e % BS) : (e / BS), rr = row_contig ? (e / BS) : (e % BS);
+      pre[q] = (J * BS + cc < n) ? L[(long long)(J * BS + cc) * rs + (long long)(i0 + rr) * cs] : T(0);
+    }
+  };
+  if (I < nblk - 1) fetch(nblk - 1);
+  for (int J = nblk - 1; J > I; --J) {
+#pragma unroll
+    for (int q = 0; q < BS * BS / kThreads; ++q) {
+      const int e = t + kThreads * q;
+      const int cc = row_contig ? (e % BS) : (e / BS), rr = row_contig ? (e / BS) : (e % BS);
+      Ls[cc][rr] = pre[q];
+    }
+    if (J - 1 > I) fetch(J - 1);
+    const unsigned need = (unsigned)(nblk - J);
+    if (t == 0 && s_known < need) s_known = wait_ready(&ctr[1], need, err);
+    __syncthreads();
+    {
+      const int jj = t >> 4, c = t & 15;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Vs[jj + 16 * q][c] = __ldcg(&Zt[(long long)(J * BS + jj + 16 * q) + c * ldy]);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int cc = 0; cc < BS; ++cc) {
+      const T l = Ls[cc][r];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] -= l * Vs[cc][g * 4 + k];
+    }
+    __syncthreads();
+  }
+  // z_I = DI_I^T acc
+#pragma unroll
+  for (int k = 0; k < 4; ++k) Vs[r][g * 4 + k] = acc[k];
+  __syncthreads();
+  const T* D = DI + (size_t)I * BS * BS;
+  T z[4] = {T(0), T(0), T(0), T(0)};
+  for (int cc = r; cc < BS; ++cc) {
+    const T d = D[cc + r * BS];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) z[k] += d * Vs[cc][g * 4 + k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c = g * 4 + k;
+    __stcg(&Zt[i + (long long)c * ldy], (i < n) ? z[k] : T(0));
+    if (i < n && c < nrhs) Z[i + (long long)c * ldz] = (VZ)((sc != nullptr) ? sc[i] * (double)z[k] : (double)z[k]);
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) st_release(&ctr[1], (unsigned)(nblk - I));
+}
+
+// ---- symmetric product A X in FP64 ----------------------------------------------
+
+// Tile task t <-> lower tile (I, J), J <= I, row-major: t = I (I + 1) / 2 + J.
+__device__ __forceinline__ void task_tile(int t, int& I, int& J) {
+  int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while (r > 0 && r * (r + 1) / 2 > t) --r;
+  while ((r + 1) * (r + 2) / 2 <= t) ++r;
+  I = r;
+  J = t - r * (r + 1) / 2;
+}
+
+// Each stored element of the lower triangle is read once: the CTA of tile (I, J)
+// writes the partial products U(I,J) = A_IJ X_J (rows of block I) and
+// V(I,J) = A_IJ^T X_I (rows of block J; on a diagonal tile only the strictly lower
+// part), each SY x NR, row-major [row][rhs].  absval: |A| instead of A.
+// Dynamic shared memory: Xi [SY][NR], S [16][SY + 1], Xc [16][NR] (FP64).
+__global__ void __launch_bounds__(kThreads)
+    symv_tiles_kernel(const double* __restrict__ a, long long rs, long long cs, int n,
+                      const double* __restrict__ X, long long ldx, int nrhs, int absval,
+                      double* __restrict__ U, double* __restrict__ V) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* Xi = reinterpret_cast<double*>(smem_raw);
+  double* S = Xi + SY * NR;
+  double* Xc = S + 16 * (SY + 1);
+  int I, J;
+  task_tile(blockIdx.x, I, J);
+  const int i0 = I * SY, j0 = J * SY, t = threadIdx.x;
+  const bool diag = (I == J), row_contig = (rs == 1);
+  for (int c = 0; c < NR; ++c) {
+    const int i = i0 + t;
+    Xi[t * NR + c] = (i < n && c < nrhs) ? X[i + (long long)c * ldx] : 0.0;
+  }
+  double u[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) u[c] = 0.0;
+  double* Vt = V + (size_t)blockIdx.x * SY * NR;
+  for (int jc = 0; jc < SY / 16; ++jc) {
+    const int jb0 = j0 + jc * 16;
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < 16; ++q) {
+      const int e = t + kThreads * q;
+      const int ii = row_contig ? (e % SY) : (e / 16), jj = row_contig ? (e / SY) : (e % 16);
+      const int i = i0 + ii, j = jb0 + jj;
+      double v = 0.0;
+      if (i < n && j < n && (!diag || i >= j)) {
+        v = a[(long long)i * rs + (long long)j * cs];
+        if (absval) v = fabs(v);
+      }
+      S[jj * (SY + 1) + ii] = v;
+    }
+    {
+      const int jj = t >> 4, c = t & 15, j = jb0 + jj;
+      Xc[jj * NR + c] = (j < n && c < nrhs) ? X[j + (long long)c * ldx] : 0.0;
+    }
+    __syncthreads();
+    // U: row t of the tile times the 16 columns of this chunk
+#pragma unroll 4
+    for (int jj = 0; jj < 16; ++jj) {
+      const double s = S[jj * (SY + 1) + t];
+#pragma unroll
+      for (int c = 0; c < NR; ++c) u[c] = fma(s, Xc[jj * NR + c], u[c]);
+    }
+    // V: column jj of the chunk (thread t: jj = t / 16, rhs c = t % 16) times X_I
+    {
+      const int jj = t >> 4, c = t & 15;
+      const double* Sc = S + jj * (SY + 1);
+      double v = 0.0;
+#pragma unroll 8
+      for (int ii = 0; ii < SY; ++ii) v = fma(Sc[ii], Xi[ii * NR + c], v);
+      if (diag) {
+        const int id = jc * 16 + jj;   // the diagonal element of this column
+        v -= Sc[id] * Xi[id * NR + c];
+      }
+      Vt[(jc * 16 + jj) * NR + c] = v;
+    }
+  }
+  double* Ut = U + (size_t)blockIdx.x * SY * NR + (size_t)t * NR;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) Ut[c] = u[c];
+}
+
+// Y_K = alpha * (sum_{J <= K} U(K,J) + sum_{I >= K} V(I,K)) + beta * B_K, summed in
+// a fixed order (deterministic).  One CTA per SY-row block, thread = row.
+// B may alias Y; ldy/ldb columns, only the first nrhs columns are written.
+__global__ void __launch_bounds__(kThreads)
+    symv_reduce_kernel(const double* __restrict__ U, const double* __restrict__ V, int n, int ntile, double alpha,
+                       double beta, const double* B, long long ldb, double* Y, long long ldy, int nrhs) {
+  const int K = blockIdx.x, t = threadIdx.x, i = K * SY + t;
+  double sum[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) sum[c] = 0.0;
+  for (int J = 0; J <= K; ++J) {
+    const double* p = U + ((size_t)(K * (K + 1) / 2 + J) * SY + t) * NR;
+#pragma unroll
+    for (int c = 0; c < NR; ++c) sum[c] += p[c];
+  }
+  for (int I = K; I < ntile; ++I) {
+    const double* p = V + ((size_t)(I * (I + 1) / 2 + K) * SY + t) * NR;
+#pragma unroll
+    for (int c = 0; c < NR; ++c) sum[c] += p[c];
+  }
+  if (i >= n) return;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) {
+    if (c < nrhs) {
+      double y = alpha * sum[c];
+      if (beta != 0.0) y += beta * B[i + (long long)c * ldb];
+      Y[i + (long long)c * ldy] = y;
+    }
+  }
+}
+
+// ---- PCG vector kernels (n x NR, column-major, leading dimension ld) ------------------
+// Deterministic reductions: each CTA writes per-RHS partials part[blockIdx.x][NR];
+// the kernel that consumes them sums all partials in the same order.
+constexpr int kVecBlocks = 256;
+
+__device__ __forceinline__ void block_sum16(double (&v)[NR], double* sh /* [kThreads][NR+1] */) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) sh[t * (NR + 1) + c] = v[c];
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if (t < s) {
+#pragma unroll
+      for (int c = 0; c < NR; ++c) sh[t * (NR + 1) + c] += sh[(t + s) * (NR + 1) + c];
+    }
+    __syncthreads();
+  }
+}
+__device__ __forceinline__ void block_max16(double (&v)[NR], double* sh) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) sh[t * (NR + 1) + c] = v[c];
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if (t < s) {
+#pragma unroll
+      for (int c = 0; c < NR; ++c) sh[t * (NR + 1) + c] = fmax(sh[t * (NR + 1) + c], sh[(t + s) * (NR + 1) + c]);
+    }
+    __syncthreads();
+  }
+}
+
+// part[b][c] = sum over this CTA's rows of a(i, c) * b(i, c)
+__global__ void __launch_bounds__(kThreads) dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                                       int n, long long ld, double* __restrict__ part) {
+  __shared__ double sh[kThreads * (NR + 1)];
+  double v[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) v[c] = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c) v[c] = fma(a[i + c * ld], b[i + c * ld], v[c]);
+  }
+  block_sum16(v, sh);
+  if (threadIdx.x < NR) part[blockIdx.x * NR + threadIdx.x] = sh[threadIdx.x];
+}
+
+__device__ __forceinline__ double sum_parts(const double* part, int nparts, int c) {
+  double s = 0.0;
+  for (int b = 0; b < nparts; ++b) s += part[b * NR + c];
+  return s;
+}
+
+// alpha_c = rz_c / (p_c . q_c); x += alpha p; r -= alpha q; partial max |r|, max |x|
+// into part_norm[b][0..NR) and [NR..2NR).
+__global__ void __launch_bounds__(kThreads)
+    update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                     const double* __restrict__ q, int n, long long ld, const double* __restrict__ part_pq,
+                     const double* __restrict__ rz, double* __restrict__ part_norm) {
+  __shared__ double alpha[NR];
+  __shared__ double sh[kThreads * (NR + 1)];
+  if (threadIdx.x < NR) {
+    const int c = threadIdx.x;
+    const double pq = sum_parts(part_pq, kVecBlocks, c);
+    alpha[c] = (pq > 0.0 && rz[c] > 0.0) ? rz[c] / pq : 0.0;
+  }
+  __syncthreads();
+  double rm[NR], xm[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) rm[c] = xm[c] = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      const double xv = fma(alpha[c], p[i + c * ld], x[i + c * ld]);
+      const double rv = fma(-alpha[c], q[i + c * ld], r[i + c * ld]);
+      x[i + c * ld] = xv;
+      r[i + c * ld] = rv;
+      rm[c] = fmax(rm[c], fabs(rv));
+      xm[c] = fmax(xm[c], fabs(xv));
+    }
+  }
+  block_max16(rm, sh);
+  if (threadIdx.x < NR) part_norm[blockIdx.x * 2 * NR + threadIdx.x] = sh[threadIdx.x];
+  __syncthreads();
+  block_max16(xm, sh);
+  if (threadIdx.x < NR) part_norm[blockIdx.x * 2 * NR + NR + threadIdx.x] = sh[threadIdx.x];
+}
+
+// partial max |a(:, c)| and max |b(:, c)| (b may be null)
+__global__ void __launch_bounds__(kThreads) norms_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                                         int n, long long ld, double* __restrict__ part_norm) {
+  __shared__ double sh[kThreads * (NR + 1)];
+  double am[NR], bm[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) am[c] = bm[c] = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      am[c] = fmax(am[c], fabs(a[i + c * ld]));
+      if (b != nullptr) bm[c] = fmax(bm[c], fabs(b[i + c * ld]));
+    }
+  }
+  block_max16(am, sh);
+  if (threadIdx.x < NR) part_norm[blockIdx.x * 2 * NR + threadIdx.x] = sh[threadIdx.x];
+  __syncthreads();
+  block_max16(bm, sh);
+  if (threadIdx.x < NR) part_norm[blockIdx.x * 2 * NR + NR + threadIdx.x] = sh[threadIdx.x];
+}
+
+// out[0..2NR) = max over the partials (one CTA)
+__global__ void norms_final_kernel(const double* __restrict__ part_norm, int nparts, double* __restrict__ out) {
+  const int c = threadIdx.x;
+  if (c >= 2 * NR) return;
+  double m = 0.0;
+  for (int b = 0; b < nparts; ++b) m = fmax(m, part_norm[b * 2 * NR + c]);
+  out[c] = m;
+}
+
+// rz_new = sum of part_rz; beta = rz_new / rz_old (0 when restart or rz_old == 0);
+// p = z + beta p.  Block 0 stores rz_new.
+__global__ void __launch_bounds__(kThreads)
+    update_p_kernel(double* __restrict__ p, const double* __restrict__ z, int n, long long ld,
+                    const double* __restrict__ part_rz, const double* __restrict__ rz_old,
+                    double* __restrict__ rz_new, int restart) {
+  __shared__ double beta[NR];
+  if (threadIdx.x < NR) {
+    const int c = threadIdx.x;
+    const double rn = sum_parts(part_rz, kVecBlocks, c);
+    beta[c] = (!restart && rz_old[c] > 0.0) ? rn / rz_old[c] : 0.0;
+    if (blockIdx.x == 0) rz_new[c] = rn;
+  }
+  __syncthreads();
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c) p[i + c * ld] = fma(beta[c], p[i + c * ld], z[i + c * ld]);
+  }
+}
+
+// dst (ld) = src (lds) for columns < ncols, zero for the rest of the NR columns
+__global__ void load_cols_kernel(const double* __restrict__ src, long long lds, int ncols, int n,
+                                 double* __restrict__ dst, long long ld) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * NR;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    dst[i + c * ld] = (c < ncols) ? src[i + c * lds] : 0.0;
+  }
+}
+__global__ void store_cols_kernel(const double* __restrict__ src, long long ld, int ncols, int n,
+                                  double* __restrict__ dst, long long ldd) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * ncols;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    dst[i + c * ldd] = src[i + c * ld];
+  }
+}
+
+}  // namespace mx
+}  // namespace
+
+// ---- host side ------------------------------------------------------------------
+
+struct __cucholmixed_st {
+  CULAPACKhandle h;
+  int precision;              // CUCHOL_MIXED_BF16 or CUCHOL_MIXED_TF32
+  int n;
+  const double* A;            // the caller's matrix (read by every residual)
+  long long rs, cs;           // its logical lower view
+  float* W;                   // FP32 factor of S A S + shift I (lower, ldw)
+  long long ldw;
+  double* s;                  // the scaling S
+  float* DI;                  // inverses of W's 64 x 64 diagonal blocks
+  double anorm;               // |A|_inf
+  double shift;               // shift of the factor that succeeded
+  double shift_request;       // caller's shift (< 0: automatic)
+  long long ld;               // rows of the work vectors
+  double *x, *r, *z, *p, *q, *b;
+  float* y;                   // triangular-solve intermediate
+  double *U, *V;              // symmetric-product partials
+  double *part, *part_norm, *rz, *norms;
+  double* h_norms;            // pinned mirror of norms
+  unsigned* ctr;              // triangular-solve counters
+  int* err;                   // a bounded wait gave up
+};
+
+namespace {
+namespace mx {
+
+inline int ntile_of(int n) { return (n + SY - 1) / SY; }
+constexpr size_t kSymvSmem = sizeof(double) * (SY * NR + 16 * (SY + 1) + 16 * NR);
+
+template <typename T>
+CUresult block_inverse(const T* L, long long rs, long long cs, int n, T* DI, cudaStream_t s) {
+  const size_t smem = 2 * sizeof(T) * BS * (BS + 1);
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(block_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    attr = true;
+  }
+  block_inverse_kernel<T><<<(n + BS - 1) / BS, BS, smem, s>>>(L, rs, cs, n, DI);
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+// Y = alpha A X + beta B for the symmetric A (one triangle, lower view rs, cs).
+CUresult symv(const double* A, long long rs, long long cs, int n, const double* X, long long ldx, int nrhs,
+              int absval, double alpha, double beta, const double* B, long long ldb, double* Y, long long ldy,
+              double* U, double* V, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(symv_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSymvSmem));
+    attr = true;
+  }
+  const int T = ntile_of(n);
+  symv_tiles_kernel<<<T * (T + 1) / 2, kThreads, kSymvSmem, s>>>(A, rs, cs, n, X, ldx, nrhs, absval, U, V);
+  CUCHOL_CHECK(cudaGetLastError());
+  symv_reduce_kernel<<<T, kThreads, 0, s>>>(U, V, n, T, alpha, beta, B, ldb, Y, ldy, nrhs);
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+// Z = S L^-T L^-1 S R (the preconditioner), 16 columns.
+CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
+  const int nblk = (p->n + BS - 1) / BS;
+  CUCHOL_CHECK(cudaMemsetAsync(p->ctr, 0, 4 * sizeof(unsigned), s));
+  trsv_fwd_kernel<float, double><<<nblk, kThreads, 0, s>>>(p->W, 1, p->ldw, p->n, p->DI, R, p->ld, p->s, p->y,
+                                                           p->ld, NR, p->ctr, p->err);
+  CUCHOL_CHECK(cudaGetLastError());
+  trsv_bwd_kernel<float, double><<<nblk, kThreads, 0, s>>>(p->W, 1, p->ldw, p->n, p->DI, p->y, p->ld, p->s, Z,
+                                                           p->ld, p->y, NR, p->ctr + 2, p->err);
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+// C := C - Q(a0 + i) Q(b0 + j)^T on the lower tiles of an m x ncols FP32 region whose
+// top-left element is on the diagonal; Q k-major (q_rows x k used, row pitch ldq).
+template <typename Op>
+CUresult tc_update(CULAPACKhandle h, const Op* q, long long ldq, int q_rows, int k, int a0, int b0, float* c,
+                   long long ldc, int m, int ncols, cudaStream_t s, const int* stop) {
+  if (m <= 0 || ncols <= 0 || k <= 0) return CUDA_SUCCESS;
+  EncodeTiledFn fn = encode_tiled();
+  if (fn == nullptr) return CUDA_ERROR_NOT_SUPPORTED;
+  CUtensorMap mq, mc;
+  const cuuint32_t es[2] = {1, 1};
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)q_rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldq * sizeof(Op)};
+    const cuuint32_t box[2] = {(cuuint32_t)tc::OpKind<Op>::BK, (cuuint32_t)tc::BM};
+    const CUtensorMapDataType dt = sizeof(Op) == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    if (fn(&mq, dt, 2, const_cast<Op*>(q), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+      return CUDA_ERROR_INVALID_VALUE;
+  }
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)ncols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldc * sizeof(float)};
+    const cuuint32_t box[2] = {32, 32};
+    if (fn(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, c, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+      return CUDA_ERROR_INVALID_VALUE;
+  }
+  tc::Params prm{};
+  prm.m = m;
+  prm.n = ncols;
+  prm.k = k;
+  prm.a_row0 = a0;
+  prm.b_row0 = b0;
+  prm.alpha = -1.f;
+  prm.lower_only = 1;
+  prm.tiles_m = (m + tc::BM - 1) / tc::BM;
+  prm.tiles_n = (ncols + tc::BN - 1) / tc::BN;
+  prm.err = h->d_words + 3;
+  const int tiles = prm.tiles_n * (prm.tiles_n + 1) / 2 + (prm.tiles_m - prm.tiles_n) * prm.tiles_n;
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(tc::update_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      tc::SMEM_BYTES));
+    attr = true;
+  }
+  tc::update_kernel<Op><<<tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(mq, mq, mc, prm, stop);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+// Blocked Cholesky of the FP32 matrix W (lower, ldw) with FP64 diagonal blocks, FP32
+// panel solves and tensor-core trailing updates in Op; schedule as ?potrf.
+// *info = first failing column (1-based) or 0.
+template <typename Op>
+CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* info) {
+  using Smem = DiagSmem<double, SB>;
+  cudaStream_t sp = h->s_panel, su = h->s_update;
+  int* d_info = h->d_words;
+  const long long ldq = OB;
+  const size_t rows = round_up((size_t)n, 128) + 128;
+  const size_t small = sizeof(double) * 2 * SB * SB + sizeof(float) * SB * SB;
+  const size_t pbytes = round_up(sizeof(float) * rows * ldq, 256), qbytes = round_up(sizeof(Op) * rows * ldq, 256);
+  CUCHOL_CHECK_CU(ensure_workspace(h, round_up(small, 256) + 2 * (pbytes + qbytes)));
+  char* ws = static_cast<char*>(h->ws);
+  double* D = reinterpret_cast<double*>(ws);
+  double* winv = D + SB * SB;
+  float* winv32 = reinterpret_cast<float*>(winv + SB * SB);
+  char* base = ws + round_up(small, 256);
+  float* P[2] = {reinterpret_cast<float*>(base), reinterpret_cast<float*>(base + pbytes)};
+  Op* Q[2] = {reinterpret_cast<Op*>(base + 2 * pbytes), reinterpret_cast<Op*>(base + 2 * pbytes + qbytes)};
+
+  CUCHOL_CHECK_CU(set_smem<double>((const void*)diag_factor_kernel<double, SB, kDiagThreads2>, Smem::bytes));
+  CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
+  CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
+  CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+  CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+  CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
+  auto at = [&](long long i, long long j) { return W + i + j * ldw; };
+
+  for (int j = 0, step = 0; j < n; j += OB, ++step) {
+    const int jB = std::min(OB, n - j);
+    const int m = n - j - jB;
+    float* Pj = P[step & 1];
+    Op* Qj = Q[step & 1];
+    const int q_rows = n - j - SB;   // P / Q row r = global row j + SB + r
+    for (int s0 = 0; s0 < jB; s0 += SB) {
+      const int c = j + s0, jb = std::min(SB, j + jB - c), mr = n - c - jb;
+      diag_in_kernel<<<jb, SB, 0, sp>>>(at(c, c), ldw, jb, D, d_info);
+      diag_factor_kernel<double, SB, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
+          D, 1, SB, jb, mr > 0 ? winv : nullptr, SB, c, d_info, h->d_logdet);
+      diag_out_kernel<<<jb, SB, 0, sp>>>(D, mr > 0 ? winv : nullptr, jb, at(c, c), ldw, winv32, d_info);
+      h->launches += 3;
+      CUCHOL_CHECK(cudaGetLastError());
+      if (mr == 0) break;
+      float* Ps = Pj + (long long)s0 * ldq + s0;
+      GemmProblem<float> t = problem<float>();
+      t.a = at(c + jb, c); t.a_rs = 1; t.a_ks = ldw;
+      t.b = winv32; t.b_rs = 1; t.b_ks = SB; t.conj_b = 1;
+      t.c = Ps; t.c_rs = ldq; t.c_cs = 1;
+      t.m = mr; t.n = jb; t.k = jb;
+      CUCHOL_CHECK_CU(gemm<float>(h, t, sp, d_info));
+      panel_store_kernel<Op><<<dim3((mr + 31) / 32, (jb + 31) / 32), 256, 0, sp>>>(
+          Ps, ldq, mr, jb, at(c + jb, c), ldw, Qj + (long long)s0 * ldq + s0, d_info);
+      ++h->launches;
+      CUCHOL_CHECK(cudaGetLastError());
+      if (s0 == 0 && jB > SB)   // the second sub-panel's columns by the first
+        CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, SB, 0, 0, at(j + SB, j + SB), ldw, n - j - SB, jB - SB,
+                                      sp, d_info));
+    }
+    CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+    if (m == 0) break;
+    const int jB2 = std::min(OB, m);
+    CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+    CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, jB, SB, SB, at(j + OB, j + OB), ldw, m, jB2, sp, d_info));
+    CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+    if (m > jB2)
+      CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, jB, SB + jB2, SB + jB2, at(j + OB + jB2, j + OB + jB2), ldw,
+                                    m - jB2, m - jB2, su, d_info));
+    CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
+  }
+  CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
+  CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, d_info, 4 * sizeof(int), cudaMemcpyDeviceToHost, sp));
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  CUCHOL_CHECK_CU(check_engine(h));
+  *info = h->h_words[0];
+  return CUDA_SUCCESS;
+}
+
+void free_mixed(CUcholMixed p) {
+  if (p == nullptr) return;
+  cudaFree(p->W);
+  cudaFree(p->s);
+  cudaFree(p->DI);
+  cudaFree(p->x);
+  cudaFree(p->y);
+  cudaFree(p->U);
+  cudaFree(p->V);
+  cudaFree(p->part);
+  cudaFree(p->ctr);
+  cudaFreeHost(p->h_norms);
+  delete p;
+}
+
+// Largest column max |v(:, c)| for c < 2 NR of the partials -> host (synchronises s).
+CUresult fetch_norms(CUcholMixed p, cudaStream_t s) {
+  norms_final_kernel<<<1, 2 * NR, 0, s>>>(p->part_norm, kVecBlocks, p->norms);
+  CUCHOL_CHECK(cudaGetLastError());
+  CUCHOL_CHECK(cudaMemcpyAsync(p->h_norms, p->norms, 2 * NR * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUCHOL_CHECK(cudaStreamSynchronize(s));
+  return CUDA_SUCCESS;
+}
+
+// Scale, |A|_inf and the low-precision factor of the plan's A (its current values).
+template <typename Op>
+CUresult mixed_refactor(CUcholMixed p, long* info) {
+  CULAPACKhandle h = p->h;
+  const int n = p->n;
+  cudaStream_t sp = h->s_panel;
+  // scaling; a non-positive diagonal entry ends the attempt (info = its row)
+  int* bad = h->d_words + 4;
+  CUCHOL_CHECK(cudaMemsetAsync(bad, 0, sizeof(int), sp));
+  scale_kernel<<<(n + 255) / 256, 256, 0, sp>>>(p->A, p->rs + p->cs, n, p->s, bad);
+  CUCHOL_CHECK(cudaGetLastError());
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words + 4, bad, sizeof(int), cudaMemcpyDeviceToHost, sp));
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  if (h->h_words[4] != 0) {
+    std::vector<double> d(n);
+    CUCHOL_CHECK(cudaMemcpy2D(d.data(), sizeof(double), p->A, (p->rs + p->cs) * sizeof(double), sizeof(double), n,
+                              cudaMemcpyDeviceToHost));
+    long k = 0;
+    while (k < n && d[k] > 0.0) ++k;
+    *info = k + 1;
+    return CUDA_SUCCESS;
+  }
+  // |A|_inf = max row sum of |A| (x is zero: column 0 set to ones)
+  CUCHOL_CHECK(cudaMemsetAsync(p->x, 0, sizeof(double) * p->ld * NR, sp));
+  {
+    std::vector<double> ones(n, 1.0);
+    CUCHOL_CHECK(cudaMemcpyAsync(p->x, ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice, sp));
+    CUCHOL_CHECK_CU(symv(p->A, p->rs, p->cs, n, p->x, p->ld, 1, 1, 1.0, 0.0, nullptr, 0, p->r, p->ld, p->U, p->V,
+                         sp));
+    CUCHOL_CHECK(cudaMemsetAsync(p->r + p->ld, 0, sizeof(double) * p->ld * (NR - 1), sp));
+    norms_kernel<<<kVecBlocks, kThreads, 0, sp>>>(p->r, nullptr, n, p->ld, p->part_norm);
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK_CU(fetch_norms(p, sp));
+    p->anorm = p->h_norms[0];
+  }
+  // factor S A S + shift I; on a breakdown retry with 8x the shift (automatic mode)
+  const double u = (sizeof(Op) == 2) ? 0x1p-8 : 0x1p-11;
+  const double shift_in = p->shift_request;
+  double shift = shift_in >= 0.0 ? shift_in : u;
+  long finfo = 0;
+  for (int attempt = 0; attempt < (shift_in >= 0.0 ? 1 : 4); ++attempt, shift *= 8.0) {
+    dim3 g((n + 31) / 32, (n + 31) / 32);
+    build_kernel<<<g, 256, 0, sp>>>(p->A, p->rs, p->cs, n, p->s, (float)shift, p->W, p->ldw);
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK_CU(mixed_factor<Op>(h, n, p->W, p->ldw, &finfo));
+    p->shift = shift;
+    if (finfo == 0) break;
+  }
+  if (finfo != 0) {
+    *info = finfo;
+    return CUDA_SUCCESS;
+  }
+  CUCHOL_CHECK_CU(block_inverse<float>(p->W, 1, p->ldw, n, p->DI, sp));
+  CUCHOL_CHECK(cudaStreamSynchronize(sp));
+  *info = 0;
+  return CUDA_SUCCESS;
+}
+
+template <typename Op>
+CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t n_, CUdeviceptr A, size_t lda,
+                      double shift_in, long* info) {
+  const int n = (int)n_;
+  auto* p = new (std::nothrow) __cucholmixed_st;
+  if (p == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
+  memset(p, 0, sizeof(*p));
+  p->h = h;
+  p->precision = (sizeof(Op) == 2) ? CUCHOL_MIXED_BF16 : CUCHOL_MIXED_TF32;
+  p->n = n;
+  p->A = reinterpret_cast<const double*>(A);
+  const bool upper = (uplo == CBlasUpper);
+  p->rs = upper ? (long long)lda : 1;
+  p->cs = upper ? 1 : (long long)lda;
+  p->ldw = (long long)round_up((size_t)n, 32);
+  p->ld = (long long)round_up((size_t)n, SY);
+  const int T = ntile_of(n), nblk = (n + BS - 1) / BS;
+  auto fail = [&](cudaError_t e) {
+    free_mixed(p);
+    return ::cuchol::report(e, "cudaMalloc", __func__, __FILE__, __LINE__);
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&p->W, sizeof(float) * p->ldw * n)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->s, sizeof(double) * n)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->DI, sizeof(float) * (size_t)nblk * BS * BS)) != cudaSuccess) return fail(e);
+  // x r z p q b in one block, then the reduction scratch
+  if ((e = cudaMalloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
+  p->r = p->x + p->ld * NR;
+  p->z = p->r + p->ld * NR;
+  p->p = p->z + p->ld * NR;
+  p->q = p->p + p->ld * NR;
+  p->b = p->q + p->ld * NR;
+  if ((e = cudaMalloc(&p->y, sizeof(float) * p->ld * NR)) != cudaSuccess) return fail(e);
+  const size_t ptile = (size_t)T * (T + 1) / 2 * SY * NR;
+  if ((e = cudaMalloc(&p->U, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->V, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->part, sizeof(double) * (kVecBlocks * NR + kVecBlocks * 2 * NR + 2 * NR + 2 * NR))) !=
+      cudaSuccess)
+    return fail(e);
+  p->part_norm = p->part + kVecBlocks * NR;
+  p->rz = p->part_norm + kVecBlocks * 2 * NR;
+  p->norms = p->rz + 2 * NR;
+  if ((e = cudaMalloc(&p->ctr, 16 * sizeof(unsigned))) != cudaSuccess) return fail(e);
+  p->err = reinterpret_cast<int*>(p->ctr + 8);
+  if ((e = cudaMemset(p->ctr, 0, 16 * sizeof(unsigned))) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocHost(&p->h_norms, 2 * NR * sizeof(double))) != cudaSuccess) return fail(e);
+
+  p->shift_request = shift_in;
+  *out = p;
+  return mixed_refactor<Op>(p, info);
+}
+
+// Preconditioned CG in FP64 on A x = b for the columns of B, 16 at a time.
+CUresult mixed_solve(CUcholMixed p, int nrhs, const double* B, long long ldb, double* X, long long ldx, double tol,
+                     int maxit, int* iter, double* berr) {
+  cudaStream_t s = p->h->s_panel;
+  const int n = p->n;
+  const long long ld = p->ld;
+  if (tol <= 0.0) tol = sqrt((double)n) * 0x1p-53;
+  if (maxit <= 0) maxit = 100;
+  int worst_it = 0;
+  bool all_ok = true;
+  double worst_berr = 0.0;
+  CUCHOL_CHECK(cudaMemsetAsync(p->err, 0, sizeof(int), s));
+  for (int g0 = 0; g0 < nrhs; g0 += NR) {
+    const int nc = std::min(NR, nrhs - g0);
+    load_cols_kernel<<<4 * p->h->num_sms, 256, 0, s>>>(B + (long long)g0 * ldb, ldb, nc, n, p->b, ld);
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK(cudaMemcpyAsync(p->r, p->b, sizeof(double) * ld * NR, cudaMemcpyDeviceToDevice, s));
+    CUCHOL_CHECK(cudaMemsetAsync(p->x, 0, sizeof(double) * ld * NR, s));
+    norms_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->b, nullptr, n, ld, p->part_norm);
+    CUCHOL_CHECK(cudaGetLastError());
+    CUCHOL_CHECK_CU(fetch_norms(p, s));
+    double bn[NR];
+    for (int c = 0; c < NR; ++c) bn[c] = p->h_norms[c];
+    auto backward = [&](const double* rx, double* eta) {   // rx: [0,NR) |r|, [NR,2NR) |x|
+      bool ok = true;
+      for (int c = 0; c < nc; ++c) {
+        const double den = p->anorm * rx[NR + c] + bn[c];
+        eta[c] = den > 0.0 ? rx[c] / den : 0.0;
+        if (!(eta[c] <= tol)) ok = false;
+      }
+      return ok;
+    };
+    double eta[NR] = {0};
+    int it = 0, slot = 0;
+    bool done = false;
+    while (!done && it < maxit) {
+      // (re)start from the current residual: p = z = M^-1 r
+      CUCHOL_CHECK_CU(precond(p, p->r, p->z, s));
+      dot_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->r, p->z, n, ld, p->part);
+      update_p_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->p, p->z, n, ld, p->part, p->rz + slot * NR,
+                                                      p->rz + (slot ^ 1) * NR, 1);
+      CUCHOL_CHECK(cudaGetLastError());
+      slot ^= 1;
+      while (it < maxit) {
+        CUCHOL_CHECK_CU(symv(p->A, p->rs, p->cs, n, p->p, ld, NR, 0, 1.0, 0.0, nullptr, 0, p->q, ld, p->U, p->V, s));
+        dot_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->p, p->q, n, ld, p->part);
+        update_xr_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->x, p->r, p->p, p->q, n, ld, p->part, p->rz + slot * NR,
+                                                         p->part_norm);
+        CUCHOL_CHECK(cudaGetLastError());
+        CUCHOL_CHECK_CU(fetch_norms(p, s));
+        ++it;
+        if (backward(p->h_norms, eta)) break;
+        CUCHOL_CHECK_CU(precond(p, p->r, p->z, s));
+        dot_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->r, p->z, n, ld, p->part);
+        update_p_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->p, p->z, n, ld, p->part, p->rz + slot * NR,
+                                                        p->rz + (slot ^ 1) * NR, 0);
+        CUCHOL_CHECK(cudaGetLastError());
+        slot ^= 1;
+      }
+      // FP64 residual from scratch: r = b - A x
+      CUCHOL_CHECK_CU(symv(p->A, p->rs, p->cs, n, p->x, ld, NR, 0, -1.0, 1.0, p->b, ld, p->r, ld, p->U, p->V, s));
+      norms_kernel<<<kVecBlocks, kThreads, 0, s>>>(p->r, p->x, n, ld, p->part_norm);
+      CUCHOL_CHECK(cudaGetLastError());
+      CUCHOL_CHECK_CU(fetch_norms(p, s));
+      done = backward(p->h_norms, eta);
+    }
+    store_cols_kernel<<<4 * p->h->num_sms, 256, 0, s>>>(p->x, ld, nc, n, X + (long long)g0 * ldx, ldx);
+    CUCHOL_CHECK(cudaGetLastError());
+    for (int c = 0; c < nc; ++c) worst_berr = std::max(worst_berr, eta[c]);
+    worst_it = std::max(worst_it, it);
+    if (!done) all_ok = false;
+  }
+  int err = 0;
+  CUCHOL_CHECK(cudaMemcpyAsync(&err, p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUCHOL_CHECK(cudaStreamSynchronize(s));
+  if (err != 0) {
+    if (errorHandler != nullptr)
+      errorHandler("triangular solve wait", __func__, __FILE__, __LINE__, (int)CUDA_ERROR_LAUNCH_TIMEOUT,
+                   &error_string);
+    return CUDA_ERROR_LAUNCH_TIMEOUT;
+  }
+  *iter = all_ok ? worst_it : -worst_it;
+  if (berr != nullptr) *berr = worst_berr;
+  return CUDA_SUCCESS;
+}
+
+// ?POTRS: B := A^-1 B from the Cholesky factor in A (lower L or upper U = L^T).
+template <typename T>
+CUresult potrs_run(CULAPACKhandle h, bool upper, int n, int nrhs, const T* A, long long lda, T* B, long long ldb) {
+  cudaStream_t s = h->s_panel;
+  const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
+  const int nblk = (n + BS - 1) / BS;
+  const long long ldy = (long long)nblk * BS;
+  const size_t di = round_up(sizeof(T) * (size_t)nblk * BS * BS, 256);
+  CUCHOL_CHECK_CU(ensure_workspace(h, di + sizeof(T) * ldy * NR));
+  T* DI = static_cast<T*>(h->ws);
+  T* Y = reinterpret_cast<T*>(static_cast<char*>(h->ws) + di);
+  unsigned* ctr = reinterpret_cast<unsigned*>(h->d_words + 8);   // words 8..11
+  int* err = h->d_words + 3;
+  CUCHOL_CHECK_CU(block_inverse<T>(A, rs, cs, n, DI, s));
+  for (int g0 = 0; g0 < nrhs; g0 += NR) {
+    const int nc = std::min(NR, nrhs - g0);
+    T* Bg = B + (long long)g0 * ldb;
+    CUCHOL_CHECK(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned), s));
+    trsv_fwd_kernel<T, T><<<nblk, kThreads, 0, s>>>(A, rs, cs, n, DI, Bg, ldb, nullptr, Y, ldy, nc, ctr, err);
+    CUCHOL_CHECK(cudaGetLastError());
+    trsv_bwd_kernel<T, T><<<nblk, kThreads, 0, s>>>(A, rs, cs, n, DI, Y, ldy, nullptr, Bg, ldb, Y, nc, ctr + 2,
+                                                    err);
+    CUCHOL_CHECK(cudaGetLastError());
+    h->launches += 2;
+  }
+  CUCHOL_CHECK(cudaMemcpyAsync(h->h_words, h->d_words, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUCHOL_CHECK(cudaStreamSynchronize(s));
+  return check_engine(h);
+}
+
+}  // namespace mx
+}  // namespace
+
+// ------------------------------------------------------------------------------
+// C ABI (include/cucholesky_ext.h)
+// ------------------------------------------------------------------------------
+namespace {
+template <typename T>
+CUresult api_potrs(const char* name, CULAPACKhandle h, CBlasUplo uplo, size_t n, size_t nrhs, CUdeviceptr A,
+                   size_t lda, CUdeviceptr B, size_t ldb, long* info) {
+  if (info == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  *info = 0;
+  if (bad_uplo(uplo)) *info = -2;
+  else if (lda < std::max<size_t>(1, n)) *info = -6;
+  else if (ldb < std::max<size_t>(1, n)) *info = -8;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla(name, -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0 || nrhs == 0) return CUDA_SUCCESS;
+  return mx::potrs_run<T>(h, uplo == CBlasUpper, (int)n, (int)nrhs, reinterpret_cast<const T*>(A), (long long)lda,
+                          reinterpret_cast<T*>(B), (long long)ldb);
+}
+}  // namespace
+
+extern "C" CUCHOL_EXPORT CUresult cuDpotrs(CULAPACKhandle h, CBlasUplo uplo, size_t n, size_t nrhs, CUdeviceptr A,
+                                           size_t lda, CUdeviceptr B, size_t ldb, long* info) {
+  return api_potrs<double>("cuDpotrs", h, uplo, n, nrhs, A, lda, B, ldb, info);
+}
+extern "C" CUCHOL_EXPORT CUresult cuSpotrs(CULAPACKhandle h, CBlasUplo uplo, size_t n, size_t nrhs, CUdeviceptr A,
+                                           size_t lda, CUdeviceptr B, size_t ldb, long* info) {
+  return api_potrs<float>("cuSpotrs", h, uplo, n, nrhs, A, lda, B, ldb, info);
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuDcholMixedCreate(CUcholMixed* plan, CULAPACKhandle h, CBlasUplo uplo, size_t n,
+                                                     CUdeviceptr A, size_t lda, int precision, double shift,
+                                                     long* info) {
+  if (plan == nullptr || info == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  *plan = nullptr;
+  *info = 0;
+  if (bad_uplo(uplo)) *info = -3;
+  else if (n == 0 || n > (size_t)INT_MAX / 2) *info = -4;
+  else if (lda < n) *info = -6;
+  else if (precision != CUCHOL_MIXED_BF16 && precision != CUCHOL_MIXED_TF32) *info = -7;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla("cuDcholMixedCreate", -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (precision == CUCHOL_MIXED_BF16) return mx::mixed_create<__nv_bfloat16>(plan, h, uplo, n, A, lda, shift, info);
+  return mx::mixed_create<float>(plan, h, uplo, n, A, lda, shift, info);
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuDcholMixedRefactor(CUcholMixed p, long* info) {
+  if (p == nullptr || info == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (p->precision == CUCHOL_MIXED_BF16) return mx::mixed_refactor<__nv_bfloat16>(p, info);
+  return mx::mixed_refactor<float>(p, info);
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuDcholMixedSolve(CUcholMixed p, size_t nrhs, CUdeviceptr B, size_t ldb,
+                                                    CUdeviceptr X, size_t ldx, double tol, int maxit, int* iter,
+                                                    double* berr) {
+  if (p == nullptr || iter == nullptr || ldb < (size_t)p->n || ldx < (size_t)p->n) return CUDA_ERROR_INVALID_VALUE;
+  *iter = 0;
+  if (nrhs == 0) return CUDA_SUCCESS;
+  return mx::mixed_solve(p, (int)nrhs, reinterpret_cast<const double*>(B), (long long)ldb,
+                         reinterpret_cast<double*>(X), (long long)ldx, tol, maxit, iter, berr);
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuCholMixedGetFactor(CUcholMixed p, CUdeviceptr* W, size_t* ldw, CUdeviceptr* s,
+                                                       double* anorm, double* shift) {
+  if (p == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (W != nullptr) *W = reinterpret_cast<CUdeviceptr>(p->W);
+  if (ldw != nullptr) *ldw = (size_t)p->ldw;
+  if (s != nullptr) *s = reinterpret_cast<CUdeviceptr>(p->s);
+  if (anorm != nullptr) *anorm = p->anorm;
+  if (shift != nullptr) *shift = p->shift;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuCholMixedDestroy(CUcholMixed p) {
+  if (p == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  cudaDeviceSynchronize();
+  mx::free_mixed(p);
+  return CUDA_SUCCESS;
+}
+
+// DSPOSV contract: iter > 0 -> refined mixed-precision solution, A unchanged;
+// iter < 0 -> FP64 fallback (-3: the low-precision factor broke down, -31: no
+// convergence within maxit), A holds the FP64 factor and info is cuDpotrf's.
+extern "C" CUCHOL_EXPORT CUresult cuDposvMixed(CULAPACKhandle h, CBlasUplo uplo, size_t n, size_t nrhs,
+                                               CUdeviceptr A, size_t lda, CUdeviceptr B, size_t ldb, CUdeviceptr X,
+                                               size_t ldx, int precision, int* iter, double* berr, long* info) {
+  if (iter == nullptr || info == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  *iter = 0;
+  *info = 0;
+  if (bad_uplo(uplo)) *info = -2;
+  else if (lda < std::max<size_t>(1, n)) *info = -6;
+  else if (ldb < std::max<size_t>(1, n)) *info = -8;
+  else if (ldx < std::max<size_t>(1, n)) *info = -10;
+  else if (precision != CUCHOL_MIXED_BF16 && precision != CUCHOL_MIXED_TF32) *info = -11;
+  if (*info != 0) {
+    if (xerbla != nullptr) xerbla("cuDposvMixed", -*info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0 || nrhs == 0) return CUDA_SUCCESS;
+  CUcholMixed p = nullptr;
+  long finfo = 0;
+  CUresult r = cuDcholMixedCreate(&p, h, uplo, n, A, lda, precision, -1.0, &finfo);
+  if (r != CUDA_SUCCESS) return r;
+  int it = 0;
+  if (finfo == 0) {
+    r = cuDcholMixedSolve(p, nrhs, B, ldb, X, ldx, 0.0, 0, &it, berr);
+    if (r != CUDA_SUCCESS) {
+      cuCholMixedDestroy(p);
+      return r;
+    }
+  }
+  cuCholMixedDestroy(p);
+  if (finfo == 0 && it > 0) {
+    *iter = it;
+    return CUDA_SUCCESS;
+  }
+  *iter = (finfo != 0) ? -3 : -31;
+  // FP64 fallback: X = B, factor A in place, solve
+  CUCHOL_CHECK(cudaMemcpy2D(reinterpret_cast<void*>(X), ldx * sizeof(double), reinterpret_cast<const void*>(B),
+                            ldb * sizeof(double), n * sizeof(double), nrhs, cudaMemcpyDeviceToDevice));
+  r = cuDpotrf(h, uplo, n, A, lda, info);
+  if (r != CUDA_SUCCESS || *info != 0) return r;
+  long pinfo = 0;
+  r = cuDpotrs(h, uplo, n, nrhs, A, lda, X, ldx, &pinfo);
+  if (berr != nullptr) *berr = -1.0;
+  return r;
+}

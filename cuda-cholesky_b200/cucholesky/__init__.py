@@ -76,6 +76,17 @@ def exported_symbols() -> list[str]:
     return names
 
 
+def extension_symbols() -> list[str]:
+    """Entry points of include/cucholesky_ext.h (no counterpart in the reference)."""
+    names = [f"cu{p}potrfLogdet" for p in "SDCZ"]
+    names += ["cuLAPACKGetLaunchCount", "cuDcholBatchedCreate", "cuScholBatchedCreate", "cuCholBatchedRun",
+              "cuCholBatchedResults", "cuCholBatchedGetBlockSize", "cuCholBatchedDestroy", "cuDlogdetNoAlloc",
+              "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
+              "cuCholMixedGetFactor",
+              "cuCholMixedDestroy", "cuDposvMixed"]
+    return names
+
+
 class Handle:
     """CULAPACKhandle bound to the current CUDA device."""
 
@@ -367,3 +378,98 @@ def pack_colmajor(mats, dtype):
     for m, o in zip(mats, off):
         out[o:o + m.size] = np.asarray(m, dtype=dtype).ravel(order="F")
     return out, off, sizes
+
+
+# ---- ?potrs and the mixed-precision solve (include/cucholesky_ext.h) -----------
+
+MIXED_BF16, MIXED_TF32 = 1, 2
+
+
+def call_potrs(h: Handle, prefix: str, uplo: str, n: int, nrhs: int, a: int, lda: int, b: int,
+               ldb: int) -> tuple[int, int]:
+    f = getattr(lib(), f"cu{prefix}potrs")
+    f.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t,
+                  C.POINTER(C.c_long)]
+    f.restype = C.c_int
+    info = C.c_long(0)
+    rc = f(h.value, _uplo(uplo), n, nrhs, a, lda, b, ldb, C.byref(info))
+    return rc, info.value
+
+
+class MixedPlan:
+    """cuDcholMixedCreate / Solve / GetFactor / Destroy on an FP64 device matrix
+    (column-major, leading dimension lda, pointer `a`).  The plan reads A again in
+    every solve: keep it unchanged while the plan lives."""
+
+    def __init__(self, h: Handle, uplo: str, n: int, a: int, lda: int, precision: int = MIXED_TF32,
+                 shift: float = -1.0):
+        L = lib()
+        L.cuDcholMixedCreate.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_size_t, C.c_uint64,
+                                         C.c_size_t, C.c_int, C.c_double, C.POINTER(C.c_long)]
+        L.cuDcholMixedCreate.restype = C.c_int
+        L.cuDcholMixedSolve.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t,
+                                        C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.cuDcholMixedSolve.restype = C.c_int
+        L.cuCholMixedGetFactor.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_size_t),
+                                           C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.cuCholMixedDestroy.argtypes = [C.c_void_p]
+        self.n = n
+        self._p = C.c_void_p()
+        info = C.c_long(0)
+        rc = L.cuDcholMixedCreate(C.byref(self._p), h.value, _uplo(uplo), n, a, lda, precision, shift,
+                                  C.byref(info))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuDcholMixedCreate", rc)
+        self.info = info.value
+
+    def refactor(self) -> int:
+        L = lib()
+        L.cuDcholMixedRefactor.argtypes = [C.c_void_p, C.POINTER(C.c_long)]
+        L.cuDcholMixedRefactor.restype = C.c_int
+        info = C.c_long(0)
+        rc = L.cuDcholMixedRefactor(self._p, C.byref(info))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuDcholMixedRefactor", rc)
+        self.info = info.value
+        return self.info
+
+    def solve(self, nrhs: int, b: int, ldb: int, x: int, ldx: int, tol: float = 0.0, maxit: int = 0):
+        it = C.c_int(0)
+        berr = C.c_double(0)
+        rc = lib().cuDcholMixedSolve(self._p, nrhs, b, ldb, x, ldx, tol, maxit, C.byref(it), C.byref(berr))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuDcholMixedSolve", rc)
+        return it.value, berr.value
+
+    def factor(self):
+        """(W device pointer, ldw, s device pointer, |A|_inf, shift)."""
+        w, s = C.c_uint64(0), C.c_uint64(0)
+        ldw = C.c_size_t(0)
+        anorm, shift = C.c_double(0), C.c_double(0)
+        lib().cuCholMixedGetFactor(self._p, C.byref(w), C.byref(ldw), C.byref(s), C.byref(anorm), C.byref(shift))
+        return w.value, ldw.value, s.value, anorm.value, shift.value
+
+    def close(self):
+        if self._p:
+            lib().cuCholMixedDestroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def call_posv_mixed(h: Handle, uplo: str, n: int, nrhs: int, a: int, lda: int, b: int, ldb: int, x: int,
+                    ldx: int, precision: int = MIXED_TF32):
+    """cuDposvMixed; returns (rc, iter, berr, info)."""
+    L = lib()
+    L.cuDposvMixed.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64,
+                               C.c_size_t, C.c_uint64, C.c_size_t, C.c_int, C.POINTER(C.c_int),
+                               C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    L.cuDposvMixed.restype = C.c_int
+    it, berr, info = C.c_int(0), C.c_double(0), C.c_long(0)
+    rc = L.cuDposvMixed(h.value, _uplo(uplo), n, nrhs, a, lda, b, ldb, x, ldx, precision, C.byref(it),
+                        C.byref(berr), C.byref(info))
+    return rc, it.value, berr.value, info.value

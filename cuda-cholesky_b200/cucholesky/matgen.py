@@ -10,6 +10,10 @@ path.
 * ``hpd_normal``    A = G G^H / n + I, G complex normal, Re/Im ~ N(0, 1/2)
 * ``sqexp_kernel``  K_ij = exp(-|x_i - x_j|^2 / (2 * 0.3^2)) + 1e-4 delta_ij,
                     x uniform in the unit cube (batched small matrices)
+* ``scaled_spd``    A = D (G G^T / n + 1e-3 I) D, G i.i.d. N(0, 1),
+                    D = diag(10^(k i / (n - 1))): kappa from ~1e3 (k = 0) to ~1e9
+                    (k = 3), the mixed-precision solve's inputs; ``scaled_spd_device``
+                    builds the same family on the GPU for large n
 """
 from __future__ import annotations
 
@@ -88,3 +92,30 @@ def _full_herm(T: np.ndarray, uplo: str) -> np.ndarray:
     F = F.copy()
     F[np.diag_indices(F.shape[0])] = F[np.diag_indices(F.shape[0])].real
     return F
+
+
+def scaled_spd(n: int, k: float, seed: int = 0) -> np.ndarray:
+    """Column-major FP64 A = D (G G^T / n + 1e-3 I) D (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, n))
+    d = 10.0 ** (k * np.arange(n) / max(n - 1, 1))
+    A = (G @ G.T / n + 1e-3 * np.eye(n)) * d[:, None] * d[None, :]
+    return np.asfortranarray(A)
+
+
+def scaled_spd_device(n: int, k: float, seed: int = 0, device: str = "cuda"):
+    """The ``scaled_spd`` family generated on the device (torch Philox normals,
+    FP64 product with torch): returns a torch tensor T of shape (n, n) whose
+    transpose is the column-major matrix (A is symmetric, so T itself is A)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    G = torch.randn((n, n), generator=g, device=device, dtype=torch.float64)
+    A = G @ G.T
+    A /= n
+    A.diagonal().add_(1e-3)
+    d = 10.0 ** (k * torch.arange(n, device=device, dtype=torch.float64) / max(n - 1, 1))
+    A *= d[:, None]
+    A *= d[None, :]
+    del G
+    return A

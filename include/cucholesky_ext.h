@@ -74,6 +74,51 @@ CUresult cuCholBatchedDestroy(CUcholBatched);
  * clears what must start at zero: calls that overlap on the GPU race. */
 CUresult cuDlogdetNoAlloc(CUdeviceptr x, size_t incx, size_t n, double *result, CUstream stream);
 
+
+/* ?POTRS: B := A^-1 B for the n x nrhs matrix B, from the Cholesky factor that
+ * cu?potrf left in A (same uplo).  LAPACK DPOTRS semantics; the reference library
+ * has no ?potrs (its SPD path stops at lapack/dpotrf.c:172 and dpotri.c:25).
+ * info = -k when argument k is invalid (XERBLA is called), 0 otherwise. */
+CUresult cuDpotrs(CULAPACKhandle, CBlasUplo, size_t, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, long *);
+CUresult cuSpotrs(CULAPACKhandle, CBlasUplo, size_t, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, long *);
+
+/* Mixed-precision SPD solve (LAPACK DSPOSV contract; no counterpart in the
+ * reference library).  The factor is computed on S A S + shift I, S = diag(A)^-1/2,
+ * in FP32 storage: FP64 diagonal blocks, FP32 panel solves, and trailing updates on
+ * the tensor cores with BF16 or TF32 operands and FP32 accumulation.  The solve is
+ * FP64 preconditioned conjugate gradients on A x = b (FP64 residuals from the
+ * caller's A) until every normwise backward error
+ *   |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf) <= tol.
+ *   cuDcholMixedCreate  scale, factor; keeps the pointer A (read by every solve, so
+ *                       leave it unchanged while the plan lives).  shift < 0 picks
+ *                       the shift automatically (u, 8u, 64u, 512u with u the
+ *                       operand unit roundoff, until the factor succeeds).
+ *                       *info > 0: A has a non-positive diagonal entry at that row,
+ *                       or the low-precision factor broke down at that column.
+ *   cuDcholMixedSolve   X := A^-1 B (n x nrhs, FP64), tol <= 0 -> sqrt(n) eps,
+ *                       maxit <= 0 -> 100 iterations per group of 16 columns;
+ *                       *iter = iterations of the slowest group, negative if some
+ *                       group did not reach tol; *berr = largest backward error.
+ *   cuDposvMixed        one call: create + solve; if the factor breaks down
+ *                       (*iter = -3) or the refinement does not converge
+ *                       (*iter = -31), A is overwritten by cuDpotrf and X comes
+ *                       from cuDpotrf + cuDpotrs (*info as cuDpotrf). */
+typedef struct __cucholmixed_st * CUcholMixed;
+#define CUCHOL_MIXED_BF16 1
+#define CUCHOL_MIXED_TF32 2
+CUresult cuDcholMixedCreate(CUcholMixed *, CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, int, double,
+                            long *);
+CUresult cuDcholMixedSolve(CUcholMixed, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, double, int, int *,
+                           double *);
+/* Scale and factor again from the current values of the plan's A (same pointer and
+ * order), reusing the plan's buffers; *info as cuDcholMixedCreate. */
+CUresult cuDcholMixedRefactor(CUcholMixed, long *);
+/* The FP32 factor W (lower, leading dimension *ldw) of S A S + shift I, the FP64
+ * scaling vector s, |A|_inf and the shift used (for checking the factor). */
+CUresult cuCholMixedGetFactor(CUcholMixed, CUdeviceptr *, size_t *, CUdeviceptr *, double *, double *);
+CUresult cuCholMixedDestroy(CUcholMixed);
+CUresult cuDposvMixed(CULAPACKhandle, CBlasUplo, size_t, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t,
+                      CUdeviceptr, size_t, int, int *, double *, long *);
 #ifdef __cplusplus
 }
 #endif
