@@ -206,8 +206,10 @@ __global__ void __launch_bounds__(kThreads)
     trsv_fwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
                     const VB* __restrict__ B, long long ldb, const double* __restrict__ sc, T* Y, long long ldy,
                     int nrhs, unsigned* ctr, int* err) {
-  __shared__ T Ls[BS][BS + 1];
-  __shared__ T Vs[BS][NR];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto Ls = reinterpret_cast<T(*)[BS + 1]>(smem_raw);           // [BS][BS + 1]
+  auto Ds = reinterpret_cast<T(*)[BS + 1]>(smem_raw + sizeof(T) * BS * (BS + 1));
+  auto Vs = reinterpret_cast<T(*)[NR]>(smem_raw + 2 * sizeof(T) * BS * (BS + 1));
   __shared__ unsigned s_I, s_known;
   const int t = threadIdx.x, r = t & (BS - 1), g = t >> 6;
   if (t == 0) {
@@ -216,6 +218,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   const int I = (int)s_I, i0 = I * BS, i = i0 + r;
+  {   // DI_I into shared memory first: the diagonal step then waits on no global load
+    const T* D = DI + (size_t)I * BS * BS;
+    for (int e = t; e < BS * BS; e += kThreads) Ds[e % BS][e / BS] = D[e];
+  }
   const bool row_contig = (rs == 1);
   T acc[4];
 #pragma unroll
@@ -266,10 +272,9 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int k = 0; k < 4; ++k) Vs[r][g * 4 + k] = acc[k];
   __syncthreads();
-  const T* D = DI + (size_t)I * BS * BS;
   T y[4] = {T(0), T(0), T(0), T(0)};
   for (int cc = 0; cc <= r; ++cc) {
-    const T d = D[r + cc * BS];
+    const T d = Ds[r][cc];
 #pragma unroll
     for (int k = 0; k < 4; ++k) y[k] += d * Vs[cc][g * 4 + k];
   }
@@ -293,8 +298,10 @@ __global__ void __launch_bounds__(kThreads)
     trsv_bwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
                     const T* Y, long long ldy, const double* __restrict__ sc, VZ* Z, long long ldz, T* Zt,
                     int nrhs, unsigned* ctr, int* err) {
-  __shared__ T Ls[BS][BS + 1];   // Ls[c][r] = L(J*BS + c, I*BS + r)
-  __shared__ T Vs[BS][NR];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto Ls = reinterpret_cast<T(*)[BS + 1]>(smem_raw);           // Ls[c][r] = L(J*BS + c, I*BS + r)
+  auto Ds = reinterpret_cast<T(*)[BS + 1]>(smem_raw + sizeof(T) * BS * (BS + 1));   // Ds[r][c] = DI_I(c, r)
+  auto Vs = reinterpret_cast<T(*)[NR]>(smem_raw + 2 * sizeof(T) * BS * (BS + 1));
   __shared__ unsigned s_I, s_known;
   const int nblk = (n + BS - 1) / BS;
   const int t = threadIdx.x, r = t & (BS - 1), g = t >> 6;
@@ -304,6 +311,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   const int I = nblk - 1 - (int)s_I, i0 = I * BS, i = i0 + r;
+  {
+    const T* D = DI + (size_t)I * BS * BS;
+    for (int e = t; e < BS * BS; e += kThreads) Ds[e / BS][e % BS] = D[e];
+  }
   const bool row_contig = (rs == 1);
   T acc[4];
 #pragma unroll
@@ -347,10 +358,9 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int k = 0; k < 4; ++k) Vs[r][g * 4 + k] = acc[k];
   __syncthreads();
-  const T* D = DI + (size_t)I * BS * BS;
   T z[4] = {T(0), T(0), T(0), T(0)};
   for (int cc = r; cc < BS; ++cc) {
-    const T d = D[cc + r * BS];
+    const T d = Ds[r][cc];
 #pragma unroll
     for (int k = 0; k < 4; ++k) z[k] += d * Vs[cc][g * 4 + k];
   }
@@ -365,6 +375,223 @@ __global__ void __launch_bounds__(kThreads)
   if (t == 0) st_release(&ctr[1], (unsigned)(nblk - I));
 }
 
+// ---- preconditioner: blocked triangular solves with inverted diagonal blocks -------
+// M^-1 r = S F^T F S r with F = the forward solve by L (the FP32 factor), done in
+// NBT-wide block steps: y_I = inv(L_II) t_I, then t_below -= L(below, I) y_I (and
+// the transposed sequence backwards).  inv(L_II) is formed once per factor, so each
+// step is two GEMVs that spread over the whole GPU: no step waits on a chain of
+// small blocks.  FP32 throughout (it is the preconditioner); 16 right-hand sides.
+constexpr int NBT = 2048;
+constexpr int GR = 64;            // rows (gemv_n) or output columns (gemv_t) per CTA
+constexpr int GMP = GR + 4;       // shared row pitch of a 64 x 64 chunk
+constexpr int GVP = NR + 4;       // shared row pitch of a vector chunk
+
+// Chunk k0.. of M (column-major, ldm): Ms[col][row] for rows [r0, r0 + 64) of
+// columns [k0, k0 + 64); out-of-range entries read as 0.
+__device__ __forceinline__ void gemv_fetch(const float* __restrict__ M, long long ldm, int rows, int cols, int r0,
+                                           int k0, float4 (&pm)[4]) {
+  const int t = threadIdx.x, f = t & 15;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int col = (t >> 4) + 16 * q, r = r0 + 4 * f, k = k0 + col;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (k < cols) {
+      const float* src = M + r + (long long)k * ldm;
+      if (r + 3 < rows) {
+        v = *reinterpret_cast<const float4*>(src);
+      } else {
+        if (r < rows) v.x = src[0];
+        if (r + 1 < rows) v.y = src[1];
+        if (r + 2 < rows) v.z = src[2];
+      }
+    }
+    pm[q] = v;
+  }
+}
+
+// out(r, c) = alpha * sum_k M(r, k) v(k, c) + beta * in(r, c), r < m, k < kk.
+// M: FP32 column-major (ldm, 16-byte aligned columns); v / in / out: FP32 column-
+// major with leading dimension ldv (in may alias out).  CTA: 64 rows; thread: 4
+// rows x 4 right-hand sides over a quarter of each 64-wide k chunk.
+__global__ void __launch_bounds__(kThreads)
+    gemv_n_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
+                  float alpha, float beta, const float* in, float* out, long long ldv) {
+  __shared__ __align__(16) float Ms[GR * GMP];
+  __shared__ __align__(16) float Vs[GR * GVP];
+  __shared__ float Red[4 * GR * NR];
+  const int t = threadIdx.x, rg = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
+  const int r0 = blockIdx.x * GR;
+  float acc[4][4] = {};
+  float4 pm[4];
+  float pv[4];
+  auto fetch_v = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + (t & 63), c = (t >> 6) + 4 * q;
+      pv[q] = (k < kk) ? v[k + (long long)c * ldv] : 0.f;
+    }
+  };
+  gemv_fetch(M, ldm, m, kk, r0, 0, pm);
+  fetch_v(0);
+  for (int k0 = 0; k0 < kk; k0 += GR) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      *reinterpret_cast<float4*>(&Ms[((t >> 4) + 16 * q) * GMP + 4 * (t & 15)]) = pm[q];
+      Vs[(t & 63) * GVP + (t >> 6) + 4 * q] = pv[q];
+    }
+    __syncthreads();
+    if (k0 + GR < kk) {
+      gemv_fetch(M, ldm, m, kk, r0, k0 + GR, pm);
+      fetch_v(k0 + GR);
+    }
+#pragma unroll
+    for (int kq = 0; kq < 16; ++kq) {
+      const int k = ks * 16 + kq;
+      const float4 a = *reinterpret_cast<const float4*>(&Ms[k * GMP + 4 * rg]);
+      const float4 b = *reinterpret_cast<const float4*>(&Vs[k * GVP + 4 * cg]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) Red[(ks * GR + 4 * rg + i) * NR + 4 * cg + j] = acc[i][j];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int row = t & 63, c = (t >> 6) * 4 + q, r = r0 + row;
+    const float sum = ((Red[(0 * GR + row) * NR + c] + Red[(1 * GR + row) * NR + c]) +
+                       (Red[(2 * GR + row) * NR + c] + Red[(3 * GR + row) * NR + c]));
+    if (r < m) {
+      float o = alpha * sum;
+      if (beta != 0.f) o = fmaf(beta, in[r + (long long)c * ldv], o);
+      out[r + (long long)c * ldv] = o;
+    }
+  }
+}
+
+// out(j, c) = alpha * sum_k M(k, j) v(k, c) + beta * in(j, c), j < m, k < kk (the
+// transposed product).  CTA: 64 output columns; the chunk is transposed into
+// shared memory so that a thread reads 4 columns with one 16-byte load.
+__global__ void __launch_bounds__(kThreads)
+    gemv_t_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
+                  float alpha, float beta, const float* in, float* out, long long ldv) {
+  __shared__ __align__(16) float Ms[GR * GMP];   // Ms[k][col]
+  __shared__ __align__(16) float Vs[GR * GVP];
+  __shared__ float Red[4 * GR * NR];
+  const int t = threadIdx.x, jg = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
+  const int j0 = blockIdx.x * GR;
+  float acc[4][4] = {};
+  float4 pm[4];
+  float pv[4];
+  auto fetch_m = [&](int k0) {   // columns j0.. (64), rows k0.. (64) of M
+    const int f = t & 15;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int col = (t >> 4) + 16 * q, j = j0 + col, k = k0 + 4 * f;
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (j < m) {
+        const float* src = M + k + (long long)j * ldm;
+        if (k + 3 < kk) {
+          x = *reinterpret_cast<const float4*>(src);
+        } else {
+          if (k < kk) x.x = src[0];
+          if (k + 1 < kk) x.y = src[1];
+          if (k + 2 < kk) x.z = src[2];
+        }
+      }
+      pm[q] = x;
+    }
+  };
+  auto fetch_v = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + (t & 63), c = (t >> 6) + 4 * q;
+      pv[q] = (k < kk) ? v[k + (long long)c * ldv] : 0.f;
+    }
+  };
+  fetch_m(0);
+  fetch_v(0);
+  for (int k0 = 0; k0 < kk; k0 += GR) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int col = (t >> 4) + 16 * q, k = 4 * (t & 15);
+      Ms[(k + 0) * GMP + col] = pm[q].x;
+      Ms[(k + 1) * GMP + col] = pm[q].y;
+      Ms[(k + 2) * GMP + col] = pm[q].z;
+      Ms[(k + 3) * GMP + col] = pm[q].w;
+      Vs[(t & 63) * GVP + (t >> 6) + 4 * q] = pv[q];
+    }
+    __syncthreads();
+    if (k0 + GR < kk) {
+      fetch_m(k0 + GR);
+      fetch_v(k0 + GR);
+    }
+#pragma unroll
+    for (int kq = 0; kq < 16; ++kq) {
+      const int k = ks * 16 + kq;
+      const float4 a = *reinterpret_cast<const float4*>(&Ms[k * GMP + 4 * jg]);
+      const float4 b = *reinterpret_cast<const float4*>(&Vs[k * GVP + 4 * cg]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) Red[(ks * GR + 4 * jg + i) * NR + 4 * cg + j] = acc[i][j];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int col = t & 63, c = (t >> 6) * 4 + q, j = j0 + col;
+    const float sum = ((Red[(0 * GR + col) * NR + c] + Red[(1 * GR + col) * NR + c]) +
+                       (Red[(2 * GR + col) * NR + c] + Red[(3 * GR + col) * NR + c]));
+    if (j < m) {
+      float o = alpha * sum;
+      if (beta != 0.f) o = fmaf(beta, in[j + (long long)c * ldv], o);
+      out[j + (long long)c * ldv] = o;
+    }
+  }
+}
+
+// t = (float)(s .* r) (NR columns)
+__global__ void scale_in_kernel(const double* __restrict__ r, const double* __restrict__ s, int n, long long ld,
+                                float* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * NR;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    out[i + c * ld] = (float)(s[i] * r[i + c * ld]);
+  }
+}
+// z = s .* (double)y
+__global__ void scale_out_kernel(const float* __restrict__ y, const double* __restrict__ s, int n, long long ld,
+                                 double* __restrict__ z) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * NR;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    z[i + c * ld] = s[i] * (double)y[i + c * ld];
+  }
+}
+
+// dst(i, j) = src(i, j) converted, for i >= j (lower) or all (full); others zero.
+template <typename S, typename D>
+__global__ void convert_kernel(const S* __restrict__ src, long long lds, D* __restrict__ dst, long long ldd, int n,
+                               int lower) {
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  for (int j = blockIdx.y * 32 + (threadIdx.x >> 5); j < min(n, blockIdx.y * 32 + 32); j += 8) {
+    if (i < n) dst[i + (long long)j * ldd] = (!lower || i >= j) ? (D)src[i + (long long)j * lds] : D(0);
+  }
+}
+
 // ---- symmetric product A X in FP64 ----------------------------------------------
 
 // Tile task t <-> lower tile (I, J), J <= I, row-major: t = I (I + 1) / 2 + J.
@@ -376,75 +603,178 @@ __device__ __forceinline__ void task_tile(int t, int& I, int& J) {
   J = t - r * (r + 1) / 2;
 }
 
-// Each stored element of the lower triangle is read once: the CTA of tile (I, J)
+// Each stored element of the triangle is read once: the CTA of lower tile (I, J)
 // writes the partial products U(I,J) = A_IJ X_J (rows of block I) and
 // V(I,J) = A_IJ^T X_I (rows of block J; on a diagonal tile only the strictly lower
 // part), each SY x NR, row-major [row][rhs].  absval: |A| instead of A.
-// Dynamic shared memory: Xi [SY][NR], S [16][SY + 1], Xc [16][NR] (FP64).
-__global__ void __launch_bounds__(kThreads)
-    symv_tiles_kernel(const double* __restrict__ a, long long rs, long long cs, int n,
-                      const double* __restrict__ X, long long ldx, int nrhs, int absval,
+// The CTA reads its tile in the stored orientation (always whole columns): for
+// lower storage T = A(I-rows, J-cols), for upper storage T = A(J-rows, I-cols) =
+// A_IJ^T, and then T X and T^T X trade places.  Columns are streamed in 16-column
+// chunks through a 3-stage cp.async ring, and both products run on the FP64 tensor
+// cores (mma.sync m16n8k4): warp w computes T X for rows [32w, 32w + 32) and a
+// partial T^T X over the same 32 rows; the 8 partials are summed in shared memory.
+// FP64 tensor-bound at 16 right-hand sides (n^2 * NR FMAs for n^2 / 2 * 8 bytes).
+constexpr int kSP = SY + 4;    // S row pitch (doubles): conflict-free fragment loads
+constexpr int kXP = NR + 4;    // Xi row pitch
+constexpr int kCP = 16 + 4;    // Xc row pitch (Xc[c][jj])
+constexpr int kStages = 3;
+constexpr size_t kSymvSmemBytes =
+    sizeof(double) * (kStages * 16 * kSP + kStages * NR * kCP + SY * kXP + 8 * 16 * NR);
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(tc::smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    symv_tiles_kernel(const double* __restrict__ a, long long lda, int upper, int n,
+                      const double* __restrict__ X, long long ldx, int nrhs, int absval, int vec16,
                       double* __restrict__ U, double* __restrict__ V) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* Xi = reinterpret_cast<double*>(smem_raw);
-  double* S = Xi + SY * NR;
-  double* Xc = S + 16 * (SY + 1);
+  double* Sr = reinterpret_cast<double*>(smem_raw);   // stage s: Sr[s][jj * kSP + ii] = T(ii, chunk col jj)
+  double* Xcr = Sr + kStages * 16 * kSP;               // stage s: Xcr[s][c * kCP + jj] = X(col block + jj, c)
+  double* Xi = Xcr + kStages * NR * kCP;               // Xi[ii * kXP + c] = X(row block + ii, c)
+  double* Vr = Xi + SY * kXP;                          // Vr[w][jj][c]: per-warp partial T^T X
   int I, J;
   task_tile(blockIdx.x, I, J);
-  const int i0 = I * SY, j0 = J * SY, t = threadIdx.x;
-  const bool diag = (I == J), row_contig = (rs == 1);
-  for (int c = 0; c < NR; ++c) {
-    const int i = i0 + t;
-    Xi[t * NR + c] = (i < n && c < nrhs) ? X[i + (long long)c * ldx] : 0.0;
+  const int rb = upper ? J : I, cb = upper ? I : J;   // row / column block of T
+  const int i0 = rb * SY, j0 = cb * SY, t = threadIdx.x;
+  const int lane = t & 31, w = t >> 5, g = lane >> 2, tq = lane & 3;
+  const bool diag = (I == J);
+  for (int e = t; e < SY * NR; e += kThreads) {
+    const int ii = e % SY, c = e / SY, i = i0 + ii;
+    Xi[ii * kXP + c] = (i < n && c < nrhs) ? X[i + (long long)c * ldx] : 0.0;
   }
-  double u[NR];
-#pragma unroll
-  for (int c = 0; c < NR; ++c) u[c] = 0.0;
-  double* Vt = V + (size_t)blockIdx.x * SY * NR;
-  for (int jc = 0; jc < SY / 16; ++jc) {
+  // chunk jc -> stage st: 16 columns x 256 rows of T, and the 16 x 16 block of X
+  auto issue = [&](int jc, int st) {
+    double* S = Sr + st * 16 * kSP;
     const int jb0 = j0 + jc * 16;
-    __syncthreads();
-#pragma unroll 4
-    for (int q = 0; q < 16; ++q) {
-      const int e = t + kThreads * q;
-      const int ii = row_contig ? (e % SY) : (e / 16), jj = row_contig ? (e / SY) : (e % 16);
-      const int i = i0 + ii, j = jb0 + jj;
-      double v = 0.0;
-      if (i < n && j < n && (!diag || i >= j)) {
-        v = a[(long long)i * rs + (long long)j * cs];
-        if (absval) v = fabs(v);
-      }
-      S[jj * (SY + 1) + ii] = v;
-    }
-    {
-      const int jj = t >> 4, c = t & 15, j = jb0 + jj;
-      Xc[jj * NR + c] = (j < n && c < nrhs) ? X[j + (long long)c * ldx] : 0.0;
-    }
-    __syncthreads();
-    // U: row t of the tile times the 16 columns of this chunk
-#pragma unroll 4
-    for (int jj = 0; jj < 16; ++jj) {
-      const double s = S[jj * (SY + 1) + t];
+    if (vec16) {
 #pragma unroll
-      for (int c = 0; c < NR; ++c) u[c] = fma(s, Xc[jj * NR + c], u[c]);
-    }
-    // V: column jj of the chunk (thread t: jj = t / 16, rhs c = t % 16) times X_I
-    {
-      const int jj = t >> 4, c = t & 15;
-      const double* Sc = S + jj * (SY + 1);
-      double v = 0.0;
-#pragma unroll 8
-      for (int ii = 0; ii < SY; ++ii) v = fma(Sc[ii], Xi[ii * NR + c], v);
-      if (diag) {
-        const int id = jc * 16 + jj;   // the diagonal element of this column
-        v -= Sc[id] * Xi[id * NR + c];
+      for (int q = 0; q < 8; ++q) {
+        const int e = t + kThreads * q;            // 16-byte piece: column e / 128, rows 2 (e % 128) ..
+        const int jj = e >> 7, ii = 2 * (e & 127), i = i0 + ii, j = jb0 + jj;
+        const int bytes = (j < n && i < n) ? (i + 1 < n ? 16 : 8) : 0;
+        cp_async16(S + jj * kSP + ii, a + (bytes ? (long long)i + (long long)j * lda : 0), bytes);
       }
-      Vt[(jc * 16 + jj) * NR + c] = v;
+    } else {
+#pragma unroll 4
+      for (int q = 0; q < 16; ++q) {
+        const int e = t + kThreads * q;
+        const int jj = e >> 8, ii = e & 255, i = i0 + ii, j = jb0 + jj;
+        const int bytes = (j < n && i < n) ? 8 : 0;
+        cp_async8(S + jj * kSP + ii, a + (bytes ? (long long)i + (long long)j * lda : 0), bytes);
+      }
+    }
+    if (t < NR * 8) {   // X block: 16 columns c of 16 rows each, 16-byte pieces (2 rows)
+      double* Xc = Xcr + st * NR * kCP;
+      const int c = t >> 3, jj = 2 * (t & 7), j = jb0 + jj;
+      if (((ldx & 1) == 0) && (((uintptr_t)X & 15) == 0)) {
+        const int bytes = (c < nrhs && j < n) ? (j + 1 < n ? 16 : 8) : 0;
+        cp_async16(Xc + c * kCP + jj, X + (bytes ? (long long)j + (long long)c * ldx : 0), bytes);
+      } else {
+        const int b0 = (c < nrhs && j < n) ? 8 : 0, b1 = (c < nrhs && j + 1 < n) ? 8 : 0;
+        cp_async8(Xc + c * kCP + jj, X + (b0 ? (long long)j + (long long)c * ldx : 0), b0);
+        cp_async8(Xc + c * kCP + jj + 1, X + (b1 ? (long long)j + 1 + (long long)c * ldx : 0), b1);
+      }
+    }
+  };
+  double u[2][2][4];
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) u[m][q][e] = 0.0;
+  double* Uo = (upper ? V : U) + (size_t)blockIdx.x * SY * NR;   // T X
+  double* Vo = (upper ? U : V) + (size_t)blockIdx.x * SY * NR;   // T^T X
+  const int r0 = 32 * w;   // this warp's rows of the tile
+  constexpr int NCH = SY / 16;
+  issue(0, 0);
+  cp_async_commit();
+  issue(1, 1);
+  cp_async_commit();
+  for (int jc = 0; jc < NCH; ++jc) {
+    const int st = jc % kStages;
+    cp_async_wait<kStages - 2>();   // chunk jc has landed (this thread's copies)
+    __syncthreads();                // ... everyone's; and stage (jc + 2) % 3 is free
+    double* S = Sr + st * 16 * kSP;
+    const double* Xc = Xcr + st * NR * kCP;
+    if (diag || absval) {   // keep the stored triangle only (the other one may hold anything)
+      for (int e = t; e < 16 * SY; e += kThreads) {
+        const int jj = e >> 8, ii = e & 255, col = jc * 16 + jj;
+        double v = S[jj * kSP + ii];
+        if (diag && (upper ? ii > col : ii < col)) v = 0.0;
+        if (absval) v = fabs(v);
+        S[jj * kSP + ii] = v;
+      }
+      __syncthreads();
+    }
+    if (jc + 2 < NCH) issue(jc + 2, (jc + 2) % kStages);
+    cp_async_commit();
+    // T X: 2 m16 tiles x 2 n8 tiles x 4 k4 steps
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      const double* Sk = S + (4 * ks + tq) * kSP + r0 + g;
+      const double b0 = Xc[g * kCP + 4 * ks + tq], b1 = Xc[(8 + g) * kCP + 4 * ks + tq];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const double a0 = Sk[16 * m], a1 = Sk[16 * m + 8];
+        cuchol::dmma::dmma_16x8x4(u[m][0], a0, a1, b0);
+        cuchol::dmma::dmma_16x8x4(u[m][1], a0, a1, b1);
+      }
+    }
+    // partial T^T X over rows r0..r0+31 (on a diagonal tile without the diagonal)
+    double v[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+#pragma unroll
+    for (int ks = 0; ks < 8; ++ks) {
+      const int ii = r0 + 4 * ks + tq;
+      double a0 = S[g * kSP + ii], a1 = S[(g + 8) * kSP + ii];
+      if (diag) {
+        if (ii == jc * 16 + g) a0 = 0.0;
+        if (ii == jc * 16 + g + 8) a1 = 0.0;
+      }
+      const double b0 = Xi[ii * kXP + g], b1 = Xi[ii * kXP + 8 + g];
+      cuchol::dmma::dmma_16x8x4(v[0], a0, a1, b0);
+      cuchol::dmma::dmma_16x8x4(v[1], a0, a1, b1);
+    }
+    // C fragment: (row g, cols 2tq, 2tq+1) and (row g + 8, same cols) of each n8 tile
+    double* Vw = Vr + w * 16 * NR;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      Vw[g * NR + 8 * q + 2 * tq] = v[q][0];
+      Vw[g * NR + 8 * q + 2 * tq + 1] = v[q][1];
+      Vw[(g + 8) * NR + 8 * q + 2 * tq] = v[q][2];
+      Vw[(g + 8) * NR + 8 * q + 2 * tq + 1] = v[q][3];
+    }
+    __syncthreads();
+    {
+      double sum = 0.0;   // thread t: output (jj = t / 16, c = t % 16), warps in order
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sum += Vr[k * 16 * NR + t];
+      Vo[(jc * 16) * NR + t] = sum;
     }
   }
-  double* Ut = U + (size_t)blockIdx.x * SY * NR + (size_t)t * NR;
+  cp_async_wait<0>();
 #pragma unroll
-  for (int c = 0; c < NR; ++c) Ut[c] = u[c];
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int row = r0 + 16 * m + g, col = 8 * q + 2 * tq;
+      Uo[row * NR + col] = u[m][q][0];
+      Uo[row * NR + col + 1] = u[m][q][1];
+      Uo[(row + 8) * NR + col] = u[m][q][2];
+      Uo[(row + 8) * NR + col + 1] = u[m][q][3];
+    }
 }
 
 // Y_K = alpha * (sum_{J <= K} U(K,J) + sum_{I >= K} V(I,K)) + beta * B_K, summed in
@@ -648,13 +978,14 @@ struct __cucholmixed_st {
   float* W;                   // FP32 factor of S A S + shift I (lower, ldw)
   long long ldw;
   double* s;                  // the scaling S
-  float* DI;                  // inverses of W's 64 x 64 diagonal blocks
+  float* Dinv;                // inverses of W's NBT x NBT diagonal blocks (ld NBT)
+  double* dwork;              // NBT x NBT FP64 block for forming them
   double anorm;               // |A|_inf
   double shift;               // shift of the factor that succeeded
   double shift_request;       // caller's shift (< 0: automatic)
   long long ld;               // rows of the work vectors
   double *x, *r, *z, *p, *q, *b;
-  float* y;                   // triangular-solve intermediate
+  float *t, *y, *zf;          // preconditioner vectors (FP32)
   double *U, *V;              // symmetric-product partials
   double *part, *part_norm, *rz, *norms;
   double* h_norms;            // pinned mirror of norms
@@ -666,7 +997,7 @@ namespace {
 namespace mx {
 
 inline int ntile_of(int n) { return (n + SY - 1) / SY; }
-constexpr size_t kSymvSmem = sizeof(double) * (SY * NR + 16 * (SY + 1) + 16 * NR);
+constexpr size_t kSymvSmem = kSymvSmemBytes;
 
 template <typename T>
 CUresult block_inverse(const T* L, long long rs, long long cs, int n, T* DI, cudaStream_t s) {
@@ -693,23 +1024,64 @@ CUresult symv(const double* A, long long rs, long long cs, int n, const double* 
     attr = true;
   }
   const int T = ntile_of(n);
-  symv_tiles_kernel<<<T * (T + 1) / 2, kThreads, kSymvSmem, s>>>(A, rs, cs, n, X, ldx, nrhs, absval, U, V);
+  const int upper = (rs != 1);
+  const long long lda = upper ? rs : cs;
+  const int vec16 = ((lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
+  symv_tiles_kernel<<<T * (T + 1) / 2, kThreads, kSymvSmem, s>>>(A, lda, upper, n, X, ldx, nrhs, absval, vec16, U,
+                                                                  V);
   CUCHOL_CHECK(cudaGetLastError());
   symv_reduce_kernel<<<T, kThreads, 0, s>>>(U, V, n, T, alpha, beta, B, ldb, Y, ldy, nrhs);
   CUCHOL_CHECK(cudaGetLastError());
   return CUDA_SUCCESS;
 }
 
-// Z = S L^-T L^-1 S R (the preconditioner), 16 columns.
+template <typename T>
+constexpr size_t trsv_smem() { return sizeof(T) * (2 * BS * (BS + 1) + BS * NR); }
+
+// Opt in to the triangular solves' shared memory (above 48 KB for FP64).
+template <typename T, typename V>
+CUresult trsv_attr() {
+  static bool done = false;
+  if (!done) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(trsv_fwd_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)trsv_smem<T>()));
+    CUCHOL_CHECK(cudaFuncSetAttribute(trsv_bwd_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)trsv_smem<T>()));
+    done = true;
+  }
+  return CUDA_SUCCESS;
+}
+
+// Z = S F^T F S R (the preconditioner; F = forward solve by the FP32 factor in
+// NBT-wide steps with the inverted diagonal blocks), 16 columns.
 CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
-  const int nblk = (p->n + BS - 1) / BS;
-  CUCHOL_CHECK(cudaMemsetAsync(p->ctr, 0, 4 * sizeof(unsigned), s));
-  trsv_fwd_kernel<float, double><<<nblk, kThreads, 0, s>>>(p->W, 1, p->ldw, p->n, p->DI, R, p->ld, p->s, p->y,
-                                                           p->ld, NR, p->ctr, p->err);
+  const int n = p->n;
+  const long long ld = p->ld, ldw = p->ldw;
+  const int nT = (n + NBT - 1) / NBT, vb = 4 * p->h->num_sms;
+  scale_in_kernel<<<vb, 256, 0, s>>>(R, p->s, n, ld, p->t);
   CUCHOL_CHECK(cudaGetLastError());
-  trsv_bwd_kernel<float, double><<<nblk, kThreads, 0, s>>>(p->W, 1, p->ldw, p->n, p->DI, p->y, p->ld, p->s, Z,
-                                                           p->ld, p->y, NR, p->ctr + 2, p->err);
+  for (int I = 0; I < nT; ++I) {
+    const int b0 = I * NBT, bI = std::min(NBT, n - b0), rest = n - b0 - bI;
+    const float* D = p->Dinv + (size_t)I * NBT * NBT;
+    gemv_n_kernel<<<(bI + GR - 1) / GR, kThreads, 0, s>>>(D, NBT, bI, bI, p->t + b0, 1.f, 0.f, nullptr, p->y + b0,
+                                                         ld);
+    if (rest > 0)
+      gemv_n_kernel<<<(rest + GR - 1) / GR, kThreads, 0, s>>>(p->W + (b0 + bI) + (long long)b0 * ldw, ldw, rest,
+                                                             bI, p->y + b0, -1.f, 1.f, p->t + b0 + bI,
+                                                             p->t + b0 + bI, ld);
+  }
+  for (int I = nT - 1; I >= 0; --I) {
+    const int b0 = I * NBT, bI = std::min(NBT, n - b0);
+    const float* D = p->Dinv + (size_t)I * NBT * NBT;
+    gemv_t_kernel<<<(bI + GR - 1) / GR, kThreads, 0, s>>>(D, NBT, bI, bI, p->y + b0, 1.f, 0.f, nullptr,
+                                                         p->zf + b0, ld);
+    if (b0 > 0)
+      gemv_t_kernel<<<(b0 + GR - 1) / GR, kThreads, 0, s>>>(p->W + b0, ldw, b0, bI, p->zf + b0, -1.f, 1.f, p->y,
+                                                           p->y, ld);
+  }
+  scale_out_kernel<<<vb, 256, 0, s>>>(p->zf, p->s, n, ld, Z);
   CUCHOL_CHECK(cudaGetLastError());
+  p->h->launches += 2 + 4 * nT;
   return CUDA_SUCCESS;
 }
 
@@ -849,9 +1221,10 @@ void free_mixed(CUcholMixed p) {
   if (p == nullptr) return;
   cudaFree(p->W);
   cudaFree(p->s);
-  cudaFree(p->DI);
+  cudaFree(p->Dinv);
+  cudaFree(p->dwork);
   cudaFree(p->x);
-  cudaFree(p->y);
+  cudaFree(p->t);
   cudaFree(p->U);
   cudaFree(p->V);
   cudaFree(p->part);
@@ -921,7 +1294,26 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
     *info = finfo;
     return CUDA_SUCCESS;
   }
-  CUCHOL_CHECK_CU(block_inverse<float>(p->W, 1, p->ldw, n, p->DI, sp));
+  // inverses of the NBT-wide diagonal blocks of the factor (zeros above the
+  // diagonal), formed in FP64 on the tensor-core ?trtri path and rounded to FP32
+  const int nT = (n + NBT - 1) / NBT;
+  for (int I = 0; I < nT; ++I) {
+    const int b0 = I * NBT, bI = std::min(NBT, n - b0);
+    float* D = p->Dinv + (size_t)I * NBT * NBT;
+    const dim3 grid((bI + 31) / 32, (bI + 31) / 32);
+    convert_kernel<float, double><<<grid, 256, 0, sp>>>(p->W + b0 + (long long)b0 * p->ldw, p->ldw, p->dwork, NBT,
+                                                        bI, 1);
+    CUCHOL_CHECK(cudaGetLastError());
+    long tinfo = 0;
+    CUCHOL_CHECK_CU(trtri_run<double>(h, false, false, bI, p->dwork, NBT, &tinfo));
+    if (tinfo != 0) {   // a zero pivot cannot come out of a successful factor
+      *info = b0 + tinfo;
+      return CUDA_SUCCESS;
+    }
+    convert_kernel<double, float><<<grid, 256, 0, sp>>>(p->dwork, NBT, D, NBT, bI, 1);
+    CUCHOL_CHECK(cudaGetLastError());
+    h->launches += 2;
+  }
   CUCHOL_CHECK(cudaStreamSynchronize(sp));
   *info = 0;
   return CUDA_SUCCESS;
@@ -943,7 +1335,7 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
   p->cs = upper ? 1 : (long long)lda;
   p->ldw = (long long)round_up((size_t)n, 32);
   p->ld = (long long)round_up((size_t)n, SY);
-  const int T = ntile_of(n), nblk = (n + BS - 1) / BS;
+  const int T = ntile_of(n);
   auto fail = [&](cudaError_t e) {
     free_mixed(p);
     return ::cuchol::report(e, "cudaMalloc", __func__, __FILE__, __LINE__);
@@ -951,7 +1343,9 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
   cudaError_t e;
   if ((e = cudaMalloc(&p->W, sizeof(float) * p->ldw * n)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&p->s, sizeof(double) * n)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->DI, sizeof(float) * (size_t)nblk * BS * BS)) != cudaSuccess) return fail(e);
+  const int nT = (n + NBT - 1) / NBT;
+  if ((e = cudaMalloc(&p->Dinv, sizeof(float) * (size_t)nT * NBT * NBT)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->dwork, sizeof(double) * (size_t)NBT * NBT)) != cudaSuccess) return fail(e);
   // x r z p q b in one block, then the reduction scratch
   if ((e = cudaMalloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
   p->r = p->x + p->ld * NR;
@@ -959,7 +1353,9 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
   p->p = p->z + p->ld * NR;
   p->q = p->p + p->ld * NR;
   p->b = p->q + p->ld * NR;
-  if ((e = cudaMalloc(&p->y, sizeof(float) * p->ld * NR)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->t, sizeof(float) * 3 * p->ld * NR)) != cudaSuccess) return fail(e);
+  p->y = p->t + p->ld * NR;
+  p->zf = p->y + p->ld * NR;
   const size_t ptile = (size_t)T * (T + 1) / 2 * SY * NR;
   if ((e = cudaMalloc(&p->U, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&p->V, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
@@ -1079,13 +1475,14 @@ CUresult potrs_run(CULAPACKhandle h, bool upper, int n, int nrhs, const T* A, lo
   unsigned* ctr = reinterpret_cast<unsigned*>(h->d_words + 8);   // words 8..11
   int* err = h->d_words + 3;
   CUCHOL_CHECK_CU(block_inverse<T>(A, rs, cs, n, DI, s));
+  CUCHOL_CHECK_CU((trsv_attr<T, T>()));
   for (int g0 = 0; g0 < nrhs; g0 += NR) {
     const int nc = std::min(NR, nrhs - g0);
     T* Bg = B + (long long)g0 * ldb;
     CUCHOL_CHECK(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned), s));
-    trsv_fwd_kernel<T, T><<<nblk, kThreads, 0, s>>>(A, rs, cs, n, DI, Bg, ldb, nullptr, Y, ldy, nc, ctr, err);
+    trsv_fwd_kernel<T, T><<<nblk, kThreads, trsv_smem<T>(), s>>>(A, rs, cs, n, DI, Bg, ldb, nullptr, Y, ldy, nc, ctr, err);
     CUCHOL_CHECK(cudaGetLastError());
-    trsv_bwd_kernel<T, T><<<nblk, kThreads, 0, s>>>(A, rs, cs, n, DI, Y, ldy, nullptr, Bg, ldb, Y, nc, ctr + 2,
+    trsv_bwd_kernel<T, T><<<nblk, kThreads, trsv_smem<T>(), s>>>(A, rs, cs, n, DI, Y, ldy, nullptr, Bg, ldb, Y, nc, ctr + 2,
                                                     err);
     CUCHOL_CHECK(cudaGetLastError());
     h->launches += 2;
