@@ -8,8 +8,8 @@
 //   1. s_i = 1 / sqrt(a_ii); W = S A S + shift * I in FP32 (lower, our own buffer):
 //      the symmetric diagonal scaling removes the row/column scaling part of
 //      kappa(A) before any rounding to low precision.
-//   2. Right-looking blocked Cholesky of W with the same two-stream schedule as
-//      ?potrf (outer blocks of 256 columns = two 128-column sub-panels, lookahead):
+//   2. Right-looking blocked Cholesky of W with the two-stream schedule of ?potrf
+//      (outer blocks of 512 columns = four 128-column sub-panels, lookahead 1):
 //        - diagonal blocks in FP64 (the ?potrf diagonal kernel on an FP64 copy),
 //        - panel solve P = W21 inv(L11)^T in FP32 (SIMT engine) into a k-major
 //          buffer, then copied into W and rounded to the operand type Q (BF16 or
@@ -33,10 +33,11 @@ namespace {
 namespace mx {
 
 constexpr int SB = 128;        // sub-panel width: FP64 diagonal blocks
-constexpr int OB = 2 * SB;     // outer block
+constexpr int OB = 4 * SB;     // outer block: trailing updates with k = 512
 constexpr int BS = 64;         // triangular-solve block
 constexpr int NR = 16;         // right-hand sides per group
 constexpr int SY = 256;        // symmetric-product tile
+constexpr int NBT = 2048;      // preconditioner block (inverted diagonal blocks)
 constexpr int kThreads = 256;
 
 // ---- factor kernels --------------------------------------------------------------
@@ -89,7 +90,7 @@ __global__ void diag_in_kernel(const float* __restrict__ W, long long ldw, int j
   if (i < jb && i >= j) D[i + j * SB] = (double)W[i + (long long)j * ldw];
 }
 
-// Factored FP64 block -> W (FP32), and the FP64 inverse -> FP32 (ld SB).
+// Factored FP64 block -> W (FP32), and the FP64 inverse (ld SB) -> FP32 (ld NBT).
 __global__ void diag_out_kernel(const double* __restrict__ D, const double* __restrict__ winv, int jb,
                                 float* __restrict__ W, long long ldw, float* __restrict__ winv32,
                                 const int* __restrict__ stop) {
@@ -97,7 +98,7 @@ __global__ void diag_out_kernel(const double* __restrict__ D, const double* __re
   const int j = blockIdx.x, i = threadIdx.x;
   if (i >= jb) return;
   if (i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
-  if (winv != nullptr) winv32[i + j * SB] = (float)winv[i + j * SB];
+  winv32[i + j * NBT] = (float)winv[i + j * SB];
 }
 
 __device__ __forceinline__ float round_tf32(float x) {
@@ -381,7 +382,6 @@ __global__ void __launch_bounds__(kThreads)
 // the transposed sequence backwards).  inv(L_II) is formed once per factor, so each
 // step is two GEMVs that spread over the whole GPU: no step waits on a chain of
 // small blocks.  FP32 throughout (it is the preconditioner); 16 right-hand sides.
-constexpr int NBT = 2048;
 constexpr int GR = 64;            // rows (gemv_n) or output columns (gemv_t) per CTA
 constexpr int GMP = GR + 4;       // shared row pitch of a 64 x 64 chunk
 constexpr int GVP = NR + 4;       // shared row pitch of a vector chunk
@@ -979,7 +979,7 @@ struct __cucholmixed_st {
   long long ldw;
   double* s;                  // the scaling S
   float* Dinv;                // inverses of W's NBT x NBT diagonal blocks (ld NBT)
-  double* dwork;              // NBT x NBT FP64 block for forming them
+  float* dtmp;                // doubling scratch (n * NBT / 4)
   double anorm;               // |A|_inf
   double shift;               // shift of the factor that succeeded
   double shift_request;       // caller's shift (< 0: automatic)
@@ -1141,20 +1141,21 @@ CUresult tc_update(CULAPACKhandle h, const Op* q, long long ldq, int q_rows, int
 // Blocked Cholesky of the FP32 matrix W (lower, ldw) with FP64 diagonal blocks, FP32
 // panel solves and tensor-core trailing updates in Op; schedule as ?potrf.
 // *info = first failing column (1-based) or 0.
+// The FP32 inverse of every 128-wide diagonal block is left in dinv (the NBT-block
+// store of the plan, ld NBT) at its place in its NBT-wide block.
 template <typename Op>
-CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* info) {
+CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, float* dinv, long* info) {
   using Smem = DiagSmem<double, SB>;
   cudaStream_t sp = h->s_panel, su = h->s_update;
   int* d_info = h->d_words;
   const long long ldq = OB;
   const size_t rows = round_up((size_t)n, 128) + 128;
-  const size_t small = sizeof(double) * 2 * SB * SB + sizeof(float) * SB * SB;
+  const size_t small = sizeof(double) * 2 * SB * SB;
   const size_t pbytes = round_up(sizeof(float) * rows * ldq, 256), qbytes = round_up(sizeof(Op) * rows * ldq, 256);
   CUCHOL_CHECK_CU(ensure_workspace(h, round_up(small, 256) + 2 * (pbytes + qbytes)));
   char* ws = static_cast<char*>(h->ws);
   double* D = reinterpret_cast<double*>(ws);
   double* winv = D + SB * SB;
-  float* winv32 = reinterpret_cast<float*>(winv + SB * SB);
   char* base = ws + round_up(small, 256);
   float* P[2] = {reinterpret_cast<float*>(base), reinterpret_cast<float*>(base + pbytes)};
   Op* Q[2] = {reinterpret_cast<Op*>(base + 2 * pbytes), reinterpret_cast<Op*>(base + 2 * pbytes + qbytes)};
@@ -1175,37 +1176,43 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* in
     const int q_rows = n - j - SB;   // P / Q row r = global row j + SB + r
     for (int s0 = 0; s0 < jB; s0 += SB) {
       const int c = j + s0, jb = std::min(SB, j + jB - c), mr = n - c - jb;
+      float* winv32 = dinv + (size_t)(c / NBT) * NBT * NBT + (c % NBT) * (1 + (long long)NBT);
       diag_in_kernel<<<jb, SB, 0, sp>>>(at(c, c), ldw, jb, D, d_info);
       diag_factor_kernel<double, SB, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
-          D, 1, SB, jb, mr > 0 ? winv : nullptr, SB, c, d_info, h->d_logdet);
-      diag_out_kernel<<<jb, SB, 0, sp>>>(D, mr > 0 ? winv : nullptr, jb, at(c, c), ldw, winv32, d_info);
+          D, 1, SB, jb, winv, SB, c, d_info, h->d_logdet);
+      diag_out_kernel<<<jb, SB, 0, sp>>>(D, winv, jb, at(c, c), ldw, winv32, d_info);
       h->launches += 3;
       CUCHOL_CHECK(cudaGetLastError());
       if (mr == 0) break;
+      // rows c + jb .. n-1 are P / Q rows s0 ..; this sub-panel's columns are s0 ..
       float* Ps = Pj + (long long)s0 * ldq + s0;
+      Op* Qs = Qj + (long long)s0 * ldq + s0;
       GemmProblem<float> t = problem<float>();
       t.a = at(c + jb, c); t.a_rs = 1; t.a_ks = ldw;
-      t.b = winv32; t.b_rs = 1; t.b_ks = SB; t.conj_b = 1;
+      t.b = winv32; t.b_rs = 1; t.b_ks = NBT; t.conj_b = 1;
       t.c = Ps; t.c_rs = ldq; t.c_cs = 1;
       t.m = mr; t.n = jb; t.k = jb;
       CUCHOL_CHECK_CU(gemm<float>(h, t, sp, d_info));
-      panel_store_kernel<Op><<<dim3((mr + 31) / 32, (jb + 31) / 32), 256, 0, sp>>>(
-          Ps, ldq, mr, jb, at(c + jb, c), ldw, Qj + (long long)s0 * ldq + s0, d_info);
+      panel_store_kernel<Op><<<dim3((mr + 31) / 32, (jb + 31) / 32), 256, 0, sp>>>(Ps, ldq, mr, jb, at(c + jb, c),
+                                                                               ldw, Qs, d_info);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
-      if (s0 == 0 && jB > SB)   // the second sub-panel's columns by the first
-        CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, SB, 0, 0, at(j + SB, j + SB), ldw, n - j - SB, jB - SB,
-                                      sp, d_info));
+      if (s0 + SB < jB)   // the outer block's remaining columns by this sub-panel
+        CUCHOL_CHECK_CU(tc_update<Op>(h, Qs, ldq, q_rows - s0, jb, 0, 0, at(c + jb, c + jb), ldw, mr,
+                                      jB - s0 - SB, sp, d_info));
     }
     CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
     if (m == 0) break;
+    // P / Q rows from global row j + OB: all sub-panels' columns (k = jB)
     const int jB2 = std::min(OB, m);
+    const Op* Qt = Qj + (long long)(OB - SB) * ldq;
+    const int t_rows = q_rows - (OB - SB);
     CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
-    CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, jB, SB, SB, at(j + OB, j + OB), ldw, m, jB2, sp, d_info));
+    CUCHOL_CHECK_CU(tc_update<Op>(h, Qt, ldq, t_rows, jB, 0, 0, at(j + OB, j + OB), ldw, m, jB2, sp, d_info));
     CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
     if (m > jB2)
-      CUCHOL_CHECK_CU(tc_update<Op>(h, Qj, ldq, q_rows, jB, SB + jB2, SB + jB2, at(j + OB + jB2, j + OB + jB2), ldw,
-                                    m - jB2, m - jB2, su, d_info));
+      CUCHOL_CHECK_CU(tc_update<Op>(h, Qt, ldq, t_rows, jB, jB2, jB2, at(j + OB + jB2, j + OB + jB2), ldw, m - jB2,
+                                    m - jB2, su, d_info));
     CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   }
   CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
@@ -1222,7 +1229,7 @@ void free_mixed(CUcholMixed p) {
   cudaFree(p->W);
   cudaFree(p->s);
   cudaFree(p->Dinv);
-  cudaFree(p->dwork);
+  cudaFree(p->dtmp);
   cudaFree(p->x);
   cudaFree(p->t);
   cudaFree(p->U);
@@ -1239,6 +1246,41 @@ CUresult fetch_norms(CUcholMixed p, cudaStream_t s) {
   CUCHOL_CHECK(cudaGetLastError());
   CUCHOL_CHECK(cudaMemcpyAsync(p->h_norms, p->norms, 2 * NR * sizeof(double), cudaMemcpyDeviceToHost, s));
   CUCHOL_CHECK(cudaStreamSynchronize(s));
+  return CUDA_SUCCESS;
+}
+
+// The doubling levels of the NBT-block inverses (see mixed_refactor); the products
+// B inv(A) of one level (at most n * NBT / 4 elements) go to the plan's scratch.
+CUresult dinv_doubling(CUcholMixed p, cudaStream_t s) {
+  const int n = p->n, nT = (n + NBT - 1) / NBT;
+  const long long ldw = p->ldw;
+  for (int sz = SB; sz < NBT; sz *= 2) {
+    std::vector<GemmProblem<float>> first, second;
+    float* tmp = p->dtmp;
+    for (int I = 0; I < nT; ++I) {
+      const int b0 = I * NBT, bI = std::min(NBT, n - b0);
+      float* D = p->Dinv + (size_t)I * NBT * NBT;
+      for (int o = 0; o + sz < bI; o += 2 * sz) {
+        const int cs = std::min(sz, bI - o - sz);
+        GemmProblem<float> t1 = problem<float>();   // T = B inv(A), cs x sz
+        t1.a = p->W + (b0 + o + sz) + (long long)(b0 + o) * ldw; t1.a_rs = 1; t1.a_ks = ldw;
+        t1.b = D + o + (long long)o * NBT; t1.b_rs = NBT; t1.b_ks = 1;
+        t1.c = tmp; t1.c_rs = 1; t1.c_cs = cs;
+        t1.m = cs; t1.n = sz; t1.k = sz;
+        GemmProblem<float> t2 = problem<float>();   // X = -inv(C) T
+        t2.a = D + (o + sz) + (long long)(o + sz) * NBT; t2.a_rs = 1; t2.a_ks = NBT;
+        t2.b = tmp; t2.b_rs = cs; t2.b_ks = 1;
+        t2.c = D + (o + sz) + (long long)o * NBT; t2.c_rs = 1; t2.c_cs = NBT;
+        t2.m = cs; t2.n = sz; t2.k = cs;
+        t2.alpha = -1.f;
+        first.push_back(t1);
+        second.push_back(t2);
+        tmp += (size_t)cs * sz;
+      }
+    }
+    CUCHOL_CHECK_CU(gemm_group<float>(p->h, first, s, nullptr));
+    CUCHOL_CHECK_CU(gemm_group<float>(p->h, second, s, nullptr));
+  }
   return CUDA_SUCCESS;
 }
 
@@ -1282,11 +1324,13 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
   const double shift_in = p->shift_request;
   double shift = shift_in >= 0.0 ? shift_in : u;
   long finfo = 0;
+  const int nT = (n + NBT - 1) / NBT;
   for (int attempt = 0; attempt < (shift_in >= 0.0 ? 1 : 4); ++attempt, shift *= 8.0) {
     dim3 g((n + 31) / 32, (n + 31) / 32);
     build_kernel<<<g, 256, 0, sp>>>(p->A, p->rs, p->cs, n, p->s, (float)shift, p->W, p->ldw);
     CUCHOL_CHECK(cudaGetLastError());
-    CUCHOL_CHECK_CU(mixed_factor<Op>(h, n, p->W, p->ldw, &finfo));
+    CUCHOL_CHECK(cudaMemsetAsync(p->Dinv, 0, sizeof(float) * (size_t)nT * NBT * NBT, sp));
+    CUCHOL_CHECK_CU(mixed_factor<Op>(h, n, p->W, p->ldw, p->Dinv, &finfo));
     p->shift = shift;
     if (finfo == 0) break;
   }
@@ -1294,26 +1338,11 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
     *info = finfo;
     return CUDA_SUCCESS;
   }
-  // inverses of the NBT-wide diagonal blocks of the factor (zeros above the
-  // diagonal), formed in FP64 on the tensor-core ?trtri path and rounded to FP32
-  const int nT = (n + NBT - 1) / NBT;
-  for (int I = 0; I < nT; ++I) {
-    const int b0 = I * NBT, bI = std::min(NBT, n - b0);
-    float* D = p->Dinv + (size_t)I * NBT * NBT;
-    const dim3 grid((bI + 31) / 32, (bI + 31) / 32);
-    convert_kernel<float, double><<<grid, 256, 0, sp>>>(p->W + b0 + (long long)b0 * p->ldw, p->ldw, p->dwork, NBT,
-                                                        bI, 1);
-    CUCHOL_CHECK(cudaGetLastError());
-    long tinfo = 0;
-    CUCHOL_CHECK_CU(trtri_run<double>(h, false, false, bI, p->dwork, NBT, &tinfo));
-    if (tinfo != 0) {   // a zero pivot cannot come out of a successful factor
-      *info = b0 + tinfo;
-      return CUDA_SUCCESS;
-    }
-    convert_kernel<double, float><<<grid, 256, 0, sp>>>(p->dwork, NBT, D, NBT, bI, 1);
-    CUCHOL_CHECK(cudaGetLastError());
-    h->launches += 2;
-  }
+  // inverses of the NBT-wide diagonal blocks of the factor, from the inverses of its
+  // 128-wide diagonal blocks (left in Dinv by the factor) by recursive doubling:
+  //   inv([A 0; B C]) = [inv(A) 0; -inv(C) B inv(A), inv(C)]
+  // one grouped launch per level and product, all NBT-blocks together (FP32).
+  CUCHOL_CHECK_CU(dinv_doubling(p, sp));
   CUCHOL_CHECK(cudaStreamSynchronize(sp));
   *info = 0;
   return CUDA_SUCCESS;
@@ -1345,7 +1374,7 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
   if ((e = cudaMalloc(&p->s, sizeof(double) * n)) != cudaSuccess) return fail(e);
   const int nT = (n + NBT - 1) / NBT;
   if ((e = cudaMalloc(&p->Dinv, sizeof(float) * (size_t)nT * NBT * NBT)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->dwork, sizeof(double) * (size_t)NBT * NBT)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&p->dtmp, sizeof(float) * (size_t)n * NBT / 4 + 256)) != cudaSuccess) return fail(e);
   // x r z p q b in one block, then the reduction scratch
   if ((e = cudaMalloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
   p->r = p->x + p->ld * NR;
