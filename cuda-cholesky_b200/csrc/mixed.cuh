@@ -90,15 +90,12 @@ __global__ void diag_in_kernel(const float* __restrict__ W, long long ldw, int j
   if (i < jb && i >= j) D[i + j * SB] = (double)W[i + (long long)j * ldw];
 }
 
-// Factored FP64 block -> W (FP32), and the FP64 inverse (ld SB) -> FP32 (ld NBT).
-__global__ void diag_out_kernel(const double* __restrict__ D, const double* __restrict__ winv, int jb,
-                                float* __restrict__ W, long long ldw, float* __restrict__ winv32,
+// Factored FP64 block -> W (FP32).
+__global__ void diag_out_kernel(const double* __restrict__ D, int jb, float* __restrict__ W, long long ldw,
                                 const int* __restrict__ stop) {
   if (*stop != 0) return;
   const int j = blockIdx.x, i = threadIdx.x;
-  if (i >= jb) return;
-  if (i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
-  winv32[i + j * NBT] = (float)winv[i + j * SB];
+  if (i < jb && i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
 }
 
 __device__ __forceinline__ float round_tf32(float x) {
@@ -137,6 +134,79 @@ __global__ void panel_store_kernel(const float* __restrict__ P, long long ldq, i
     if (r < mr && q < jb) W[r + (long long)q * ldw] = t[tx][ty + 8 * k];
   }
 }
+
+// Panel solve X = B L^-T in place, row-parallel: B (m x jb, jb <= 128, logical view
+// B(i, j) = B[i*brs + j*bcs]) is overwritten by X, and X also goes to out2 (k-major
+// rows, pitch ld2, converted by to_op2).  L: the factored jb x jb diagonal block
+// (view strides lrs, lcs).  CTA: 64 rows; thread (r, cg) holds columns
+// [32cg, 32cg + 32) of row r in registers.  Column block b is solved by the threads
+// with cg == b (forward substitution, right-looking inside the block), published
+// through shared memory, and subtracted by the threads with cg > b.  Computes in T.
+template <typename T, typename TB, typename TL, typename O2>
+__global__ void __launch_bounds__(kThreads, 2)
+    trsm_rows_kernel(TB* __restrict__ B, long long brs, long long bcs, int m, int jb, const TL* __restrict__ L,
+                     long long lrs, long long lcs, O2* __restrict__ out2, long long ld2,
+                     const int* __restrict__ stop) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: L(32b + j, 32b + k)
+  T* Xs = Ls + 128 * 33;                    // [64][33]: solved block
+  T* rd = Xs + 64 * 33;                     // [32]: 1 / L(32b + j, 32b + j)
+  if (*stop != 0) return;
+  const int t = threadIdx.x, r = t & 63, cg = t >> 6;
+  const int row = blockIdx.x * 64 + r;
+  T x[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int col = cg * 32 + k;
+    x[k] = (row < m && col < jb) ? (T)B[(long long)row * brs + (long long)col * bcs] : T(0);
+  }
+  const int nblk = (jb + 31) / 32;
+  for (int b = 0; b < nblk; ++b) {
+    const int rows = 128 - 32 * b;   // rows of L from 32b down (zero past jb)
+    __syncthreads();
+    for (int e = t; e < rows * 32; e += kThreads) {
+      const int j = e >> 5, kk = e & 31;
+      const int gi = 32 * b + j, gk = 32 * b + kk;
+      Ls[j * 33 + kk] = (gi < jb && gk < jb && gi >= gk) ? (T)L[(long long)gi * lrs + (long long)gk * lcs] : T(0);
+    }
+    __syncthreads();
+    if (t < 32) rd[t] = (32 * b + t < jb) ? T(1) / Ls[t * 33 + t] : T(0);
+    __syncthreads();
+    if (cg == b) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        x[j] *= rd[j];
+#pragma unroll
+        for (int kk = j + 1; kk < 32; ++kk) x[kk] -= Ls[kk * 33 + j] * x[j];
+      }
+#pragma unroll
+      for (int kk = 0; kk < 32; ++kk) Xs[r * 33 + kk] = x[kk];
+    }
+    __syncthreads();
+    if (cg > b) {
+      const T* Lb = Ls + (cg - b) * 32 * 33;
+#pragma unroll 4
+      for (int kk = 0; kk < 32; ++kk) {
+        const T xk = Xs[r * 33 + kk];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) x[j] -= Lb[j * 33 + kk] * xk;
+      }
+    }
+  }
+  if (row < m) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const int col = cg * 32 + k;
+      if (col < jb) {
+        B[(long long)row * brs + (long long)col * bcs] = (TB)x[k];
+        out2[(long long)row * ld2 + col] = to_op<O2>((float)x[k]);
+      }
+    }
+  }
+}
+
+template <typename T>
+constexpr size_t trsm_rows_smem() { return sizeof(T) * (128 * 33 + 64 * 33 + 32); }
 
 // ---- triangular solves ------------------------------------------------------------
 
@@ -1144,21 +1214,24 @@ CUresult tc_update(CULAPACKhandle h, const Op* q, long long ldq, int q_rows, int
 // The FP32 inverse of every 128-wide diagonal block is left in dinv (the NBT-block
 // store of the plan, ld NBT) at its place in its NBT-wide block.
 template <typename Op>
-CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, float* dinv, long* info) {
+CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* info) {
   using Smem = DiagSmem<double, SB>;
   cudaStream_t sp = h->s_panel, su = h->s_update;
   int* d_info = h->d_words;
   const long long ldq = OB;
   const size_t rows = round_up((size_t)n, 128) + 128;
-  const size_t small = sizeof(double) * 2 * SB * SB;
-  const size_t pbytes = round_up(sizeof(float) * rows * ldq, 256), qbytes = round_up(sizeof(Op) * rows * ldq, 256);
-  CUCHOL_CHECK_CU(ensure_workspace(h, round_up(small, 256) + 2 * (pbytes + qbytes)));
+  const size_t small = round_up(sizeof(double) * SB * SB, 256);
+  const size_t qbytes = round_up(sizeof(Op) * rows * ldq, 256);
+  CUCHOL_CHECK_CU(ensure_workspace(h, small + 2 * qbytes));
   char* ws = static_cast<char*>(h->ws);
   double* D = reinterpret_cast<double*>(ws);
-  double* winv = D + SB * SB;
-  char* base = ws + round_up(small, 256);
-  float* P[2] = {reinterpret_cast<float*>(base), reinterpret_cast<float*>(base + pbytes)};
-  Op* Q[2] = {reinterpret_cast<Op*>(base + 2 * pbytes), reinterpret_cast<Op*>(base + 2 * pbytes + qbytes)};
+  Op* Q[2] = {reinterpret_cast<Op*>(ws + small), reinterpret_cast<Op*>(ws + small + qbytes)};
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(trsm_rows_kernel<float, float, double, Op>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_rows_smem<float>()));
+    attr = true;
+  }
 
   CUCHOL_CHECK_CU(set_smem<double>((const void*)diag_factor_kernel<double, SB, kDiagThreads2>, Smem::bytes));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
@@ -1171,30 +1244,21 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, float* d
   for (int j = 0, step = 0; j < n; j += OB, ++step) {
     const int jB = std::min(OB, n - j);
     const int m = n - j - jB;
-    float* Pj = P[step & 1];
     Op* Qj = Q[step & 1];
     const int q_rows = n - j - SB;   // P / Q row r = global row j + SB + r
     for (int s0 = 0; s0 < jB; s0 += SB) {
       const int c = j + s0, jb = std::min(SB, j + jB - c), mr = n - c - jb;
-      float* winv32 = dinv + (size_t)(c / NBT) * NBT * NBT + (c % NBT) * (1 + (long long)NBT);
       diag_in_kernel<<<jb, SB, 0, sp>>>(at(c, c), ldw, jb, D, d_info);
       diag_factor_kernel<double, SB, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
-          D, 1, SB, jb, winv, SB, c, d_info, h->d_logdet);
-      diag_out_kernel<<<jb, SB, 0, sp>>>(D, winv, jb, at(c, c), ldw, winv32, d_info);
+          D, 1, SB, jb, nullptr, SB, c, d_info, h->d_logdet);
+      diag_out_kernel<<<jb, SB, 0, sp>>>(D, jb, at(c, c), ldw, d_info);
       h->launches += 3;
       CUCHOL_CHECK(cudaGetLastError());
       if (mr == 0) break;
-      // rows c + jb .. n-1 are P / Q rows s0 ..; this sub-panel's columns are s0 ..
-      float* Ps = Pj + (long long)s0 * ldq + s0;
+      // panel rows c + jb .. n-1 solved in place; they are Q rows s0 .., columns s0 ..
       Op* Qs = Qj + (long long)s0 * ldq + s0;
-      GemmProblem<float> t = problem<float>();
-      t.a = at(c + jb, c); t.a_rs = 1; t.a_ks = ldw;
-      t.b = winv32; t.b_rs = 1; t.b_ks = NBT; t.conj_b = 1;
-      t.c = Ps; t.c_rs = ldq; t.c_cs = 1;
-      t.m = mr; t.n = jb; t.k = jb;
-      CUCHOL_CHECK_CU(gemm<float>(h, t, sp, d_info));
-      panel_store_kernel<Op><<<dim3((mr + 31) / 32, (jb + 31) / 32), 256, 0, sp>>>(Ps, ldq, mr, jb, at(c + jb, c),
-                                                                               ldw, Qs, d_info);
+      trsm_rows_kernel<float, float, double, Op><<<(mr + 63) / 64, kThreads, trsm_rows_smem<float>(), sp>>>(
+          at(c + jb, c), 1, ldw, mr, jb, D, 1, SB, Qs, ldq, d_info);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (s0 + SB < jB)   // the outer block's remaining columns by this sub-panel
@@ -1329,8 +1393,7 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
     dim3 g((n + 31) / 32, (n + 31) / 32);
     build_kernel<<<g, 256, 0, sp>>>(p->A, p->rs, p->cs, n, p->s, (float)shift, p->W, p->ldw);
     CUCHOL_CHECK(cudaGetLastError());
-    CUCHOL_CHECK(cudaMemsetAsync(p->Dinv, 0, sizeof(float) * (size_t)nT * NBT * NBT, sp));
-    CUCHOL_CHECK_CU(mixed_factor<Op>(h, n, p->W, p->ldw, p->Dinv, &finfo));
+    CUCHOL_CHECK_CU(mixed_factor<Op>(h, n, p->W, p->ldw, &finfo));
     p->shift = shift;
     if (finfo == 0) break;
   }
@@ -1338,10 +1401,23 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
     *info = finfo;
     return CUDA_SUCCESS;
   }
-  // inverses of the NBT-wide diagonal blocks of the factor, from the inverses of its
-  // 128-wide diagonal blocks (left in Dinv by the factor) by recursive doubling:
+  // inverses of the NBT-wide diagonal blocks of the factor: the 128-wide diagonal
+  // blocks inverted in place (one CTA each), then recursive doubling
   //   inv([A 0; B C]) = [inv(A) 0; -inv(C) B inv(A), inv(C)]
-  // one grouped launch per level and product, all NBT-blocks together (FP32).
+  // with one grouped launch per level and product, all NBT-blocks together (FP32).
+  CUCHOL_CHECK(cudaMemsetAsync(p->Dinv, 0, sizeof(float) * (size_t)nT * NBT * NBT, sp));
+  CUCHOL_CHECK_CU(set_smem<float>((const void*)diag_invert_kernel<float, SB, kDiagThreads2>,
+                                  DiagSmem<float, SB>::bytes));
+  for (int I = 0; I < nT; ++I) {
+    const int b0 = I * NBT, bI = std::min(NBT, n - b0);
+    float* Dn = p->Dinv + (size_t)I * NBT * NBT;
+    CUCHOL_CHECK_CU(copy_view<float>(h, p->W + b0 + (long long)b0 * p->ldw, 1, p->ldw, Dn, 1, NBT, bI, bI, true, sp,
+                                     nullptr));
+    diag_invert_kernel<float, SB, kDiagThreads2><<<(bI + SB - 1) / SB, kDiagThreads2, DiagSmem<float, SB>::bytes,
+                                                   sp>>>(Dn, 1, NBT, bI, SB, 0);
+    ++h->launches;
+    CUCHOL_CHECK(cudaGetLastError());
+  }
   CUCHOL_CHECK_CU(dinv_doubling(p, sp));
   CUCHOL_CHECK(cudaStreamSynchronize(sp));
   *info = 0;
