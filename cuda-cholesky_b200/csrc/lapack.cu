@@ -17,6 +17,7 @@
 #include "gemm.cuh"
 #include "handle.h"
 #include "panel.cuh"
+#include "trsm.cuh"
 
 using namespace cuchol;
 
@@ -321,6 +322,11 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * NB};
 
   CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_factor_kernel<T, nb, kDiagThreads2>, Smem::bytes));
+  // real types: the panel solve is a row-parallel triangular solve (no inverse of the
+  // diagonal block); complex types: inverse W, then P = A21 W^H on the GEMM engine
+  constexpr bool kReal = std::is_same<T, double>::value || std::is_same<T, float>::value;
+  if constexpr (kReal)
+    CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, false>, trsm_rows_smem<T>()));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
   CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
   // the update stream starts after the panel stream's initialisation
@@ -351,22 +357,31 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
       const int c = j + s0, jb = std::min(nb, j + jB - c);
       const int mr = n - c - jb;                 // rows below this diagonal block
       diag_factor_kernel<T, nb, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
-          at(c, c), rs, cs, jb, mr > 0 ? winv : nullptr, nb, c, d_info, h->d_logdet);
+          at(c, c), rs, cs, jb, (mr > 0 && !kReal) ? winv : nullptr, nb, c, d_info, h->d_logdet);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (mr == 0) break;
       // panel solve into P: rows c + jb .. n-1 are P rows s0 .. (P starts at j + nb)
       T* Ps = P + s0 + (long long)s0 * ldp;
-      GemmProblem<T> t = problem<T>();
-      t.a = at(c + jb, c); t.a_rs = rs; t.a_ks = cs;
-      t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;   // zeros above W's diagonal
-      t.c = Ps; t.c_rs = 1; t.c_cs = ldp;
-      t.m = mr; t.n = jb; t.k = jb;
-      CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
-      CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
-      // update stream: the solved rows into A, off the panel stream's critical path
-      CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
-      CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
+      if constexpr (kReal) {
+        // row-parallel triangular solve: A21 := A21 L11^-T in place, and into P
+        trsm_rows_kernel<T, T, T, T, false><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
+            at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
+        ++h->launches;
+        CUCHOL_CHECK(cudaGetLastError());
+        CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+      } else {
+        GemmProblem<T> t = problem<T>();
+        t.a = at(c + jb, c); t.a_rs = rs; t.a_ks = cs;
+        t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;   // zeros above W's diagonal
+        t.c = Ps; t.c_rs = 1; t.c_cs = ldp;
+        t.m = mr; t.n = jb; t.k = jb;
+        CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
+        CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+        // update stream: the solved rows into A, off the panel stream's critical path
+        CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
+        CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
+      }
       if (s0 == 0 && jB > nb) {
         // the second sub-panel's columns (rows j + nb ..) by the first sub-panel
         CUCHOL_CHECK_CU(update(j + nb, j + nb, n - j - nb, jB - nb, P, P, nb, sp));
@@ -379,7 +394,8 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
     const T* Pt = P + nb;
     CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
     CUCHOL_CHECK_CU(update(j + NB, j + NB, m, jB2, Pt, Pt, jB, sp));
-    // rest of the trailing matrix
+    // rest of the trailing matrix, once P holds both sub-panels
+    CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
     if (m > jB2) CUCHOL_CHECK_CU(update(j + NB + jB2, j + NB + jB2, m - jB2, m - jB2, Pt + jB2, Pt + jB2, jB, su));
     // always recorded: it also covers the copies that still read P
     CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));

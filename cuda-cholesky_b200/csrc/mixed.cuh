@@ -98,116 +98,6 @@ __global__ void diag_out_kernel(const double* __restrict__ D, int jb, float* __r
   if (i < jb && i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
 }
 
-__device__ __forceinline__ float round_tf32(float x) {
-  uint32_t u;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-  return __uint_as_float(u);
-}
-template <typename Op> __device__ __forceinline__ Op to_op(float x);
-template <> __device__ __forceinline__ __nv_bfloat16 to_op<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
-template <> __device__ __forceinline__ float to_op<float>(float x) { return round_tf32(x); }
-
-// Solved panel rows (k-major FP32 P, row pitch ldq) -> W (column-major) and the
-// tensor-core operand Q (k-major, rounded to BF16 or TF32).  32 x 32 tiles.
-template <typename Op>
-__global__ void panel_store_kernel(const float* __restrict__ P, long long ldq, int mr, int jb,
-                                   float* __restrict__ W, long long ldw, Op* __restrict__ Q,
-                                   const int* __restrict__ stop) {
-  if (*stop != 0) return;
-  __shared__ float t[32][33];
-  const int r0 = blockIdx.x * 32, q0 = blockIdx.y * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int r = r0 + ty + 8 * k, q = q0 + tx;
-    float v = 0.f;
-    if (r < mr && q < jb) {
-      v = P[(long long)r * ldq + q];
-      Q[(long long)r * ldq + q] = to_op<Op>(v);
-    }
-    t[ty + 8 * k][tx] = v;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int q = q0 + ty + 8 * k, r = r0 + tx;
-    if (r < mr && q < jb) W[r + (long long)q * ldw] = t[tx][ty + 8 * k];
-  }
-}
-
-// Panel solve X = B L^-T in place, row-parallel: B (m x jb, jb <= 128, logical view
-// B(i, j) = B[i*brs + j*bcs]) is overwritten by X, and X also goes to out2 (k-major
-// rows, pitch ld2, converted by to_op2).  L: the factored jb x jb diagonal block
-// (view strides lrs, lcs).  CTA: 64 rows; thread (r, cg) holds columns
-// [32cg, 32cg + 32) of row r in registers.  Column block b is solved by the threads
-// with cg == b (forward substitution, right-looking inside the block), published
-// through shared memory, and subtracted by the threads with cg > b.  Computes in T.
-template <typename T, typename TB, typename TL, typename O2>
-__global__ void __launch_bounds__(kThreads, 2)
-    trsm_rows_kernel(TB* __restrict__ B, long long brs, long long bcs, int m, int jb, const TL* __restrict__ L,
-                     long long lrs, long long lcs, O2* __restrict__ out2, long long ld2,
-                     const int* __restrict__ stop) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: L(32b + j, 32b + k)
-  T* Xs = Ls + 128 * 33;                    // [64][33]: solved block
-  T* rd = Xs + 64 * 33;                     // [32]: 1 / L(32b + j, 32b + j)
-  if (*stop != 0) return;
-  const int t = threadIdx.x, r = t & 63, cg = t >> 6;
-  const int row = blockIdx.x * 64 + r;
-  T x[32];
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    const int col = cg * 32 + k;
-    x[k] = (row < m && col < jb) ? (T)B[(long long)row * brs + (long long)col * bcs] : T(0);
-  }
-  const int nblk = (jb + 31) / 32;
-  for (int b = 0; b < nblk; ++b) {
-    const int rows = 128 - 32 * b;   // rows of L from 32b down (zero past jb)
-    __syncthreads();
-    for (int e = t; e < rows * 32; e += kThreads) {
-      const int j = e >> 5, kk = e & 31;
-      const int gi = 32 * b + j, gk = 32 * b + kk;
-      Ls[j * 33 + kk] = (gi < jb && gk < jb && gi >= gk) ? (T)L[(long long)gi * lrs + (long long)gk * lcs] : T(0);
-    }
-    __syncthreads();
-    if (t < 32) rd[t] = (32 * b + t < jb) ? T(1) / Ls[t * 33 + t] : T(0);
-    __syncthreads();
-    if (cg == b) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        x[j] *= rd[j];
-#pragma unroll
-        for (int kk = j + 1; kk < 32; ++kk) x[kk] -= Ls[kk * 33 + j] * x[j];
-      }
-#pragma unroll
-      for (int kk = 0; kk < 32; ++kk) Xs[r * 33 + kk] = x[kk];
-    }
-    __syncthreads();
-    if (cg > b) {
-      const T* Lb = Ls + (cg - b) * 32 * 33;
-#pragma unroll 4
-      for (int kk = 0; kk < 32; ++kk) {
-        const T xk = Xs[r * 33 + kk];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] -= Lb[j * 33 + kk] * xk;
-      }
-    }
-  }
-  if (row < m) {
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const int col = cg * 32 + k;
-      if (col < jb) {
-        B[(long long)row * brs + (long long)col * bcs] = (TB)x[k];
-        out2[(long long)row * ld2 + col] = to_op<O2>((float)x[k]);
-      }
-    }
-  }
-}
-
-template <typename T>
-constexpr size_t trsm_rows_smem() { return sizeof(T) * (128 * 33 + 64 * 33 + 32); }
-
 // ---- triangular solves ------------------------------------------------------------
 
 // Inverse of the 64 x 64 diagonal blocks of a lower-triangular L (logical view
@@ -456,181 +346,158 @@ constexpr int GR = 64;            // rows (gemv_n) or output columns (gemv_t) pe
 constexpr int GMP = GR + 4;       // shared row pitch of a 64 x 64 chunk
 constexpr int GVP = NR + 4;       // shared row pitch of a vector chunk
 
-// Chunk k0.. of M (column-major, ldm): Ms[col][row] for rows [r0, r0 + 64) of
-// columns [k0, k0 + 64); out-of-range entries read as 0.
-__device__ __forceinline__ void gemv_fetch(const float* __restrict__ M, long long ldm, int rows, int cols, int r0,
-                                           int k0, float4 (&pm)[4]) {
-  const int t = threadIdx.x, f = t & 15;
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(tc::smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16_(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+constexpr int GST = 4;                                  // cp.async stages
+constexpr int GSTAGE = GR * GMP + GR * GVP;             // floats per stage
+constexpr size_t kGemvSmem = sizeof(float) * (GST * GSTAGE + 4 * GR * NR);
+
+// The 4 partial 4 x 4 blocks of every thread -> out (alpha, beta), rows/columns
+// [o0, o0 + 64) of the output.
+__device__ __forceinline__ void gemv_finish(float (&acc)[4][4], float* Red, int ig, int cg, int ks, int o0, int m,
+                                            float alpha, float beta, const float* in, float* out, long long ldv) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) Red[(ks * GR + 4 * ig + i) * NR + 4 * cg + j] = acc[i][j];
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int col = (t >> 4) + 16 * q, r = r0 + 4 * f, k = k0 + col;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (k < cols) {
-      const float* src = M + r + (long long)k * ldm;
-      if (r + 3 < rows) {
-        v = *reinterpret_cast<const float4*>(src);
-      } else {
-        if (r < rows) v.x = src[0];
-        if (r + 1 < rows) v.y = src[1];
-        if (r + 2 < rows) v.z = src[2];
-      }
+    const int o = t & 63, c = (t >> 6) * 4 + q, r = o0 + o;
+    const float sum = ((Red[(0 * GR + o) * NR + c] + Red[(1 * GR + o) * NR + c]) +
+                       (Red[(2 * GR + o) * NR + c] + Red[(3 * GR + o) * NR + c]));
+    if (r < m) {
+      float v = alpha * sum;
+      if (beta != 0.f) v = fmaf(beta, in[r + (long long)c * ldv], v);
+      out[r + (long long)c * ldv] = v;
     }
-    pm[q] = v;
+  }
+}
+
+// 16 consecutive k of the stage: thread block (ig, cg) += A4(ig rows) x V4(cg rhs).
+__device__ __forceinline__ void gemv_mac(const float* Ms, const float* Vs, int ig, int cg, int ks,
+                                         float (&acc)[4][4]) {
+#pragma unroll
+  for (int kq = 0; kq < 16; ++kq) {
+    const int k = ks * 16 + kq;
+    const float4 a = *reinterpret_cast<const float4*>(&Ms[k * GMP + 4 * ig]);
+    const float4 b = *reinterpret_cast<const float4*>(&Vs[k * GVP + 4 * cg]);
+    const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+  }
+}
+
+// v chunk k0.. (64 x 16) -> Vs[k][c], zero past kk
+__device__ __forceinline__ void gemv_issue_v(float* Vs, const float* v, long long ldv, int kk, int k0) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = t + kThreads * q, k = e & 63, c = e >> 6, gk = k0 + k;
+    cp_async4(&Vs[k * GVP + c], v + (gk < kk ? gk + (long long)c * ldv : 0), gk < kk ? 4 : 0);
   }
 }
 
 // out(r, c) = alpha * sum_k M(r, k) v(k, c) + beta * in(r, c), r < m, k < kk.
-// M: FP32 column-major (ldm, 16-byte aligned columns); v / in / out: FP32 column-
-// major with leading dimension ldv (in may alias out).  CTA: 64 rows; thread: 4
-// rows x 4 right-hand sides over a quarter of each 64-wide k chunk.
+// M: FP32 column-major (ldm a multiple of 4, 16-byte aligned columns); v / in / out:
+// FP32 column-major with leading dimension ldv (in may alias out).  CTA: 64 rows;
+// M and v stream through a 4-stage cp.async ring in 64-wide k chunks (each column
+// segment of 64 rows = 16 pieces of 16 bytes, stored as Ms[k][row]); thread: 4 rows
+// x 4 right-hand sides over a quarter of each chunk.
 __global__ void __launch_bounds__(kThreads)
     gemv_n_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
                   float alpha, float beta, const float* in, float* out, long long ldv) {
-  __shared__ __align__(16) float Ms[GR * GMP];
-  __shared__ __align__(16) float Vs[GR * GVP];
-  __shared__ float Red[4 * GR * NR];
-  const int t = threadIdx.x, rg = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* ring = reinterpret_cast<float*>(smem_raw);
+  float* Red = ring + GST * GSTAGE;
+  const int t = threadIdx.x, ig = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
   const int r0 = blockIdx.x * GR;
-  float acc[4][4] = {};
-  float4 pm[4];
-  float pv[4];
-  auto fetch_v = [&](int k0) {
+  const int nch = (kk + GR - 1) / GR;
+  auto issue = [&](int ch) {
+    float* Ms = ring + (ch % GST) * GSTAGE;
+    float* Vs = Ms + GR * GMP;
+    const int k0 = ch * GR;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int k = k0 + (t & 63), c = (t >> 6) + 4 * q;
-      pv[q] = (k < kk) ? v[k + (long long)c * ldv] : 0.f;
+    for (int q = 0; q < 4; ++q) {   // 16-byte piece f of column col: rows r0 + 4f ..
+      const int e = t + kThreads * q, f = e & 15, col = e >> 4, r = r0 + 4 * f, k = k0 + col;
+      const float* src = M + r + (long long)k * ldm;
+      int bytes = 0;
+      if (k < kk && r < m) bytes = (r + 3 < m) ? 16 : 4 * (m - r);
+      cp_async16_(&Ms[col * GMP + 4 * f], bytes ? src : M, bytes);
     }
+    gemv_issue_v(Vs, v, ldv, kk, k0);
   };
-  gemv_fetch(M, ldm, m, kk, r0, 0, pm);
-  fetch_v(0);
-  for (int k0 = 0; k0 < kk; k0 += GR) {
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      *reinterpret_cast<float4*>(&Ms[((t >> 4) + 16 * q) * GMP + 4 * (t & 15)]) = pm[q];
-      Vs[(t & 63) * GVP + (t >> 6) + 4 * q] = pv[q];
-    }
-    __syncthreads();
-    if (k0 + GR < kk) {
-      gemv_fetch(M, ldm, m, kk, r0, k0 + GR, pm);
-      fetch_v(k0 + GR);
-    }
-#pragma unroll
-    for (int kq = 0; kq < 16; ++kq) {
-      const int k = ks * 16 + kq;
-      const float4 a = *reinterpret_cast<const float4*>(&Ms[k * GMP + 4 * rg]);
-      const float4 b = *reinterpret_cast<const float4*>(&Vs[k * GVP + 4 * cg]);
-      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-    }
+  float acc[4][4] = {};
+  for (int ch = 0; ch < GST - 1; ++ch) {
+    if (ch < nch) issue(ch);
+    cp_async_commit();
   }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) Red[(ks * GR + 4 * rg + i) * NR + 4 * cg + j] = acc[i][j];
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int row = t & 63, c = (t >> 6) * 4 + q, r = r0 + row;
-    const float sum = ((Red[(0 * GR + row) * NR + c] + Red[(1 * GR + row) * NR + c]) +
-                       (Red[(2 * GR + row) * NR + c] + Red[(3 * GR + row) * NR + c]));
-    if (r < m) {
-      float o = alpha * sum;
-      if (beta != 0.f) o = fmaf(beta, in[r + (long long)c * ldv], o);
-      out[r + (long long)c * ldv] = o;
-    }
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait<GST - 2>();
+    __syncthreads();
+    if (ch + GST - 1 < nch) issue(ch + GST - 1);
+    cp_async_commit();
+    const float* Ms = ring + (ch % GST) * GSTAGE;
+    gemv_mac(Ms, Ms + GR * GMP, ig, cg, ks, acc);
   }
+  cp_async_wait<0>();
+  gemv_finish(acc, Red, ig, cg, ks, r0, m, alpha, beta, in, out, ldv);
 }
 
 // out(j, c) = alpha * sum_k M(k, j) v(k, c) + beta * in(j, c), j < m, k < kk (the
-// transposed product).  CTA: 64 output columns; the chunk is transposed into
-// shared memory so that a thread reads 4 columns with one 16-byte load.
+// transposed product).  CTA: 64 output columns; the chunk is transposed on its way
+// into shared memory (4-byte copies, Ms[k][col]) so that a thread reads 4 columns
+// with one 16-byte load.
 __global__ void __launch_bounds__(kThreads)
     gemv_t_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
                   float alpha, float beta, const float* in, float* out, long long ldv) {
-  __shared__ __align__(16) float Ms[GR * GMP];   // Ms[k][col]
-  __shared__ __align__(16) float Vs[GR * GVP];
-  __shared__ float Red[4 * GR * NR];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* ring = reinterpret_cast<float*>(smem_raw);
+  float* Red = ring + GST * GSTAGE;
   const int t = threadIdx.x, jg = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
   const int j0 = blockIdx.x * GR;
+  const int nch = (kk + GR - 1) / GR;
+  auto issue = [&](int ch) {
+    float* Ms = ring + (ch % GST) * GSTAGE;
+    float* Vs = Ms + GR * GMP;
+    const int k0 = ch * GR;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {   // element (k, col): consecutive threads, consecutive k
+      const int e = t + kThreads * q, k = e & 63, col = e >> 6, gk = k0 + k, j = j0 + col;
+      const bool ok = gk < kk && j < m;
+      cp_async4(&Ms[k * GMP + col], ok ? M + gk + (long long)j * ldm : M, ok ? 4 : 0);
+    }
+    gemv_issue_v(Vs, v, ldv, kk, k0);
+  };
   float acc[4][4] = {};
-  float4 pm[4];
-  float pv[4];
-  auto fetch_m = [&](int k0) {   // columns j0.. (64), rows k0.. (64) of M
-    const int f = t & 15;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int col = (t >> 4) + 16 * q, j = j0 + col, k = k0 + 4 * f;
-      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (j < m) {
-        const float* src = M + k + (long long)j * ldm;
-        if (k + 3 < kk) {
-          x = *reinterpret_cast<const float4*>(src);
-        } else {
-          if (k < kk) x.x = src[0];
-          if (k + 1 < kk) x.y = src[1];
-          if (k + 2 < kk) x.z = src[2];
-        }
-      }
-      pm[q] = x;
-    }
-  };
-  auto fetch_v = [&](int k0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int k = k0 + (t & 63), c = (t >> 6) + 4 * q;
-      pv[q] = (k < kk) ? v[k + (long long)c * ldv] : 0.f;
-    }
-  };
-  fetch_m(0);
-  fetch_v(0);
-  for (int k0 = 0; k0 < kk; k0 += GR) {
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int col = (t >> 4) + 16 * q, k = 4 * (t & 15);
-      Ms[(k + 0) * GMP + col] = pm[q].x;
-      Ms[(k + 1) * GMP + col] = pm[q].y;
-      Ms[(k + 2) * GMP + col] = pm[q].z;
-      Ms[(k + 3) * GMP + col] = pm[q].w;
-      Vs[(t & 63) * GVP + (t >> 6) + 4 * q] = pv[q];
-    }
-    __syncthreads();
-    if (k0 + GR < kk) {
-      fetch_m(k0 + GR);
-      fetch_v(k0 + GR);
-    }
-#pragma unroll
-    for (int kq = 0; kq < 16; ++kq) {
-      const int k = ks * 16 + kq;
-      const float4 a = *reinterpret_cast<const float4*>(&Ms[k * GMP + 4 * jg]);
-      const float4 b = *reinterpret_cast<const float4*>(&Vs[k * GVP + 4 * cg]);
-      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-    }
+  for (int ch = 0; ch < GST - 1; ++ch) {
+    if (ch < nch) issue(ch);
+    cp_async_commit();
   }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) Red[(ks * GR + 4 * jg + i) * NR + 4 * cg + j] = acc[i][j];
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int col = t & 63, c = (t >> 6) * 4 + q, j = j0 + col;
-    const float sum = ((Red[(0 * GR + col) * NR + c] + Red[(1 * GR + col) * NR + c]) +
-                       (Red[(2 * GR + col) * NR + c] + Red[(3 * GR + col) * NR + c]));
-    if (j < m) {
-      float o = alpha * sum;
-      if (beta != 0.f) o = fmaf(beta, in[j + (long long)c * ldv], o);
-      out[j + (long long)c * ldv] = o;
-    }
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait<GST - 2>();
+    __syncthreads();
+    if (ch + GST - 1 < nch) issue(ch + GST - 1);
+    cp_async_commit();
+    const float* Ms = ring + (ch % GST) * GSTAGE;
+    gemv_mac(Ms, Ms + GR * GMP, jg, cg, ks, acc);
   }
+  cp_async_wait<0>();
+  gemv_finish(acc, Red, jg, cg, ks, j0, m, alpha, beta, in, out, ldv);
 }
 
 // t = (float)(s .* r) (NR columns)
@@ -698,11 +565,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_b
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(tc::smem_u32(dst)), "l"(src), "r"(src_bytes)
                : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -1125,6 +987,12 @@ CUresult trsv_attr() {
 // Z = S F^T F S R (the preconditioner; F = forward solve by the FP32 factor in
 // NBT-wide steps with the inverted diagonal blocks), 16 columns.
 CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(gemv_n_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemvSmem));
+    CUCHOL_CHECK(cudaFuncSetAttribute(gemv_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemvSmem));
+    attr = true;
+  }
   const int n = p->n;
   const long long ld = p->ld, ldw = p->ldw;
   const int nT = (n + NBT - 1) / NBT, vb = 4 * p->h->num_sms;
@@ -1133,20 +1001,20 @@ CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
   for (int I = 0; I < nT; ++I) {
     const int b0 = I * NBT, bI = std::min(NBT, n - b0), rest = n - b0 - bI;
     const float* D = p->Dinv + (size_t)I * NBT * NBT;
-    gemv_n_kernel<<<(bI + GR - 1) / GR, kThreads, 0, s>>>(D, NBT, bI, bI, p->t + b0, 1.f, 0.f, nullptr, p->y + b0,
+    gemv_n_kernel<<<(bI + GR - 1) / GR, kThreads, kGemvSmem, s>>>(D, NBT, bI, bI, p->t + b0, 1.f, 0.f, nullptr, p->y + b0,
                                                          ld);
     if (rest > 0)
-      gemv_n_kernel<<<(rest + GR - 1) / GR, kThreads, 0, s>>>(p->W + (b0 + bI) + (long long)b0 * ldw, ldw, rest,
+      gemv_n_kernel<<<(rest + GR - 1) / GR, kThreads, kGemvSmem, s>>>(p->W + (b0 + bI) + (long long)b0 * ldw, ldw, rest,
                                                              bI, p->y + b0, -1.f, 1.f, p->t + b0 + bI,
                                                              p->t + b0 + bI, ld);
   }
   for (int I = nT - 1; I >= 0; --I) {
     const int b0 = I * NBT, bI = std::min(NBT, n - b0);
     const float* D = p->Dinv + (size_t)I * NBT * NBT;
-    gemv_t_kernel<<<(bI + GR - 1) / GR, kThreads, 0, s>>>(D, NBT, bI, bI, p->y + b0, 1.f, 0.f, nullptr,
+    gemv_t_kernel<<<(bI + GR - 1) / GR, kThreads, kGemvSmem, s>>>(D, NBT, bI, bI, p->y + b0, 1.f, 0.f, nullptr,
                                                          p->zf + b0, ld);
     if (b0 > 0)
-      gemv_t_kernel<<<(b0 + GR - 1) / GR, kThreads, 0, s>>>(p->W + b0, ldw, b0, bI, p->zf + b0, -1.f, 1.f, p->y,
+      gemv_t_kernel<<<(b0 + GR - 1) / GR, kThreads, kGemvSmem, s>>>(p->W + b0, ldw, b0, bI, p->zf + b0, -1.f, 1.f, p->y,
                                                            p->y, ld);
   }
   scale_out_kernel<<<vb, 256, 0, s>>>(p->zf, p->s, n, ld, Z);
@@ -1228,7 +1096,7 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* in
   Op* Q[2] = {reinterpret_cast<Op*>(ws + small), reinterpret_cast<Op*>(ws + small + qbytes)};
   static bool attr = false;
   if (!attr) {
-    CUCHOL_CHECK(cudaFuncSetAttribute(trsm_rows_kernel<float, float, double, Op>,
+    CUCHOL_CHECK(cudaFuncSetAttribute(trsm_rows_kernel<float, float, double, Op, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_rows_smem<float>()));
     attr = true;
   }
@@ -1257,8 +1125,8 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* in
       if (mr == 0) break;
       // panel rows c + jb .. n-1 solved in place; they are Q rows s0 .., columns s0 ..
       Op* Qs = Qj + (long long)s0 * ldq + s0;
-      trsm_rows_kernel<float, float, double, Op><<<(mr + 63) / 64, kThreads, trsm_rows_smem<float>(), sp>>>(
-          at(c + jb, c), 1, ldw, mr, jb, D, 1, SB, Qs, ldq, d_info);
+      trsm_rows_kernel<float, float, double, Op, true><<<(mr + 63) / 64, kThreads, trsm_rows_smem<float>(), sp>>>(
+          at(c + jb, c), 1, ldw, mr, jb, D, 1, SB, Qs, ldq, 1, d_info);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (s0 + SB < jB)   // the outer block's remaining columns by this sub-panel
