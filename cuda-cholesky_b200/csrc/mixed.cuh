@@ -364,9 +364,11 @@ constexpr int GSTAGE = GR * GMP + GR * GVP;             // floats per stage
 constexpr size_t kGemvSmem = sizeof(float) * (GST * GSTAGE + 4 * GR * NR);
 
 // The 4 partial 4 x 4 blocks of every thread -> out (alpha, beta), rows/columns
-// [o0, o0 + 64) of the output.
+// [o0, o0 + 64) of the output; with a split k range (part != null) the raw sums go to
+// part[o][c] of this split instead, for gemv_reduce_kernel.
 __device__ __forceinline__ void gemv_finish(float (&acc)[4][4], float* Red, int ig, int cg, int ks, int o0, int m,
-                                            float alpha, float beta, const float* in, float* out, long long ldv) {
+                                            float alpha, float beta, const float* in, float* out, long long ldv,
+                                            float* part) {
   const int t = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -378,12 +380,27 @@ __device__ __forceinline__ void gemv_finish(float (&acc)[4][4], float* Red, int 
     const int o = t & 63, c = (t >> 6) * 4 + q, r = o0 + o;
     const float sum = ((Red[(0 * GR + o) * NR + c] + Red[(1 * GR + o) * NR + c]) +
                        (Red[(2 * GR + o) * NR + c] + Red[(3 * GR + o) * NR + c]));
-    if (r < m) {
+    if (part != nullptr) {
+      part[(long long)r * NR + c] = sum;
+    } else if (r < m) {
       float v = alpha * sum;
       if (beta != 0.f) v = fmaf(beta, in[r + (long long)c * ldv], v);
       out[r + (long long)c * ldv] = v;
     }
   }
+}
+
+// out(r, c) = alpha * sum_s part[s][r][c] + beta * in(r, c), the splits in order.
+__global__ void gemv_reduce_kernel(const float* __restrict__ part, int nsplit, long long mp, int m, float alpha,
+                                   float beta, const float* in, float* out, long long ldv) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)m * NR) return;
+  const int r = (int)(e / NR), c = (int)(e % NR);
+  float sum = 0.f;
+  for (int q = 0; q < nsplit; ++q) sum += part[((long long)q * mp + r) * NR + c];
+  float v = alpha * sum;
+  if (beta != 0.f) v = fmaf(beta, in[r + (long long)c * ldv], v);
+  out[r + (long long)c * ldv] = v;
 }
 
 // 16 consecutive k of the stage: thread block (ig, cg) += A4(ig rows) x V4(cg rhs).
@@ -420,26 +437,28 @@ __device__ __forceinline__ void gemv_issue_v(float* Vs, const float* v, long lon
 // x 4 right-hand sides over a quarter of each chunk.
 __global__ void __launch_bounds__(kThreads)
     gemv_n_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
-                  float alpha, float beta, const float* in, float* out, long long ldv) {
+                  float alpha, float beta, const float* in, float* out, long long ldv, int kc, float* part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* ring = reinterpret_cast<float*>(smem_raw);
   float* Red = ring + GST * GSTAGE;
   const int t = threadIdx.x, ig = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
   const int r0 = blockIdx.x * GR;
-  const int nch = (kk + GR - 1) / GR;
+  // this CTA's k range [kb, ke): split blockIdx.y of width kc (a multiple of 64)
+  const int kb = blockIdx.y * kc, ke = min(kk, kb + kc);
+  const int nch = (ke - kb + GR - 1) / GR;
   auto issue = [&](int ch) {
     float* Ms = ring + (ch % GST) * GSTAGE;
     float* Vs = Ms + GR * GMP;
-    const int k0 = ch * GR;
+    const int k0 = kb + ch * GR;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {   // 16-byte piece f of column col: rows r0 + 4f ..
       const int e = t + kThreads * q, f = e & 15, col = e >> 4, r = r0 + 4 * f, k = k0 + col;
       const float* src = M + r + (long long)k * ldm;
       int bytes = 0;
-      if (k < kk && r < m) bytes = (r + 3 < m) ? 16 : 4 * (m - r);
+      if (k < ke && r < m) bytes = (r + 3 < m) ? 16 : 4 * (m - r);
       cp_async16_(&Ms[col * GMP + 4 * f], bytes ? src : M, bytes);
     }
-    gemv_issue_v(Vs, v, ldv, kk, k0);
+    gemv_issue_v(Vs, v, ldv, ke, k0);
   };
   float acc[4][4] = {};
   for (int ch = 0; ch < GST - 1; ++ch) {
@@ -455,7 +474,8 @@ __global__ void __launch_bounds__(kThreads)
     gemv_mac(Ms, Ms + GR * GMP, ig, cg, ks, acc);
   }
   cp_async_wait<0>();
-  gemv_finish(acc, Red, ig, cg, ks, r0, m, alpha, beta, in, out, ldv);
+  gemv_finish(acc, Red, ig, cg, ks, r0, m, alpha, beta, in, out, ldv,
+              part ? part + (long long)blockIdx.y * gridDim.x * GR * NR : nullptr);
 }
 
 // out(j, c) = alpha * sum_k M(k, j) v(k, c) + beta * in(j, c), j < m, k < kk (the
@@ -464,24 +484,25 @@ __global__ void __launch_bounds__(kThreads)
 // with one 16-byte load.
 __global__ void __launch_bounds__(kThreads)
     gemv_t_kernel(const float* __restrict__ M, long long ldm, int m, int kk, const float* __restrict__ v,
-                  float alpha, float beta, const float* in, float* out, long long ldv) {
+                  float alpha, float beta, const float* in, float* out, long long ldv, int kc, float* part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* ring = reinterpret_cast<float*>(smem_raw);
   float* Red = ring + GST * GSTAGE;
   const int t = threadIdx.x, jg = t & 15, cg = (t >> 4) & 3, ks = t >> 6;
   const int j0 = blockIdx.x * GR;
-  const int nch = (kk + GR - 1) / GR;
+  const int kb = blockIdx.y * kc, ke = min(kk, kb + kc);
+  const int nch = (ke - kb + GR - 1) / GR;
   auto issue = [&](int ch) {
     float* Ms = ring + (ch % GST) * GSTAGE;
     float* Vs = Ms + GR * GMP;
-    const int k0 = ch * GR;
+    const int k0 = kb + ch * GR;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {   // element (k, col): consecutive threads, consecutive k
       const int e = t + kThreads * q, k = e & 63, col = e >> 6, gk = k0 + k, j = j0 + col;
-      const bool ok = gk < kk && j < m;
+      const bool ok = gk < ke && j < m;
       cp_async4(&Ms[k * GMP + col], ok ? M + gk + (long long)j * ldm : M, ok ? 4 : 0);
     }
-    gemv_issue_v(Vs, v, ldv, kk, k0);
+    gemv_issue_v(Vs, v, ldv, ke, k0);
   };
   float acc[4][4] = {};
   for (int ch = 0; ch < GST - 1; ++ch) {
@@ -497,7 +518,8 @@ __global__ void __launch_bounds__(kThreads)
     gemv_mac(Ms, Ms + GR * GMP, jg, cg, ks, acc);
   }
   cp_async_wait<0>();
-  gemv_finish(acc, Red, jg, cg, ks, j0, m, alpha, beta, in, out, ldv);
+  gemv_finish(acc, Red, jg, cg, ks, j0, m, alpha, beta, in, out, ldv,
+              part ? part + (long long)blockIdx.y * gridDim.x * GR * NR : nullptr);
 }
 
 // t = (float)(s .* r) (NR columns)
@@ -912,6 +934,7 @@ struct __cucholmixed_st {
   double* s;                  // the scaling S
   float* Dinv;                // inverses of W's NBT x NBT diagonal blocks (ld NBT)
   float* dtmp;                // doubling scratch (n * NBT / 4)
+  float* gpart;               // split-k partial sums of the preconditioner GEMVs
   double anorm;               // |A|_inf
   double shift;               // shift of the factor that succeeded
   double shift_request;       // caller's shift (< 0: automatic)
@@ -996,30 +1019,50 @@ CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
   const int n = p->n;
   const long long ld = p->ld, ldw = p->ldw;
   const int nT = (n + NBT - 1) / NBT, vb = 4 * p->h->num_sms;
+  // one GEMV; with fewer than two CTAs per SM the k range is split (chunks of 256 or
+  // more) and the partial sums reduced in order by a second launch
+  auto gemv = [&](bool trans, const float* M, long long ldm, int m, int kk, const float* v, float alpha,
+                  float beta, const float* in, float* out) -> CUresult {
+    const int blocks = (m + GR - 1) / GR, want = 2 * p->h->num_sms;
+    int split = 1;
+    if (blocks < want) split = std::max(1, std::min((want + blocks - 1) / blocks, kk / 256));
+    const int kc = (int)round_up((size_t)((kk + split - 1) / split), GR);
+    split = (kk + kc - 1) / kc;
+    float* part = split > 1 ? p->gpart : nullptr;
+    const dim3 grid(blocks, split);
+    if (trans)
+      gemv_t_kernel<<<grid, kThreads, kGemvSmem, s>>>(M, ldm, m, kk, v, alpha, beta, in, out, ld, kc, part);
+    else
+      gemv_n_kernel<<<grid, kThreads, kGemvSmem, s>>>(M, ldm, m, kk, v, alpha, beta, in, out, ld, kc, part);
+    CUCHOL_CHECK(cudaGetLastError());
+    ++p->h->launches;
+    if (split > 1) {
+      gemv_reduce_kernel<<<(m * NR + 255) / 256, 256, 0, s>>>(part, split, (long long)blocks * GR, m, alpha, beta,
+                                                              in, out, ld);
+      CUCHOL_CHECK(cudaGetLastError());
+      ++p->h->launches;
+    }
+    return CUDA_SUCCESS;
+  };
   scale_in_kernel<<<vb, 256, 0, s>>>(R, p->s, n, ld, p->t);
   CUCHOL_CHECK(cudaGetLastError());
   for (int I = 0; I < nT; ++I) {
     const int b0 = I * NBT, bI = std::min(NBT, n - b0), rest = n - b0 - bI;
     const float* D = p->Dinv + (size_t)I * NBT * NBT;
-    gemv_n_kernel<<<(bI + GR - 1) / GR, kThreads, kGemvSmem, s>>>(D, NBT, bI, bI, p->t + b0, 1.f, 0.f, nullptr, p->y + b0,
-                                                         ld);
+    CUCHOL_CHECK_CU(gemv(false, D, NBT, bI, bI, p->t + b0, 1.f, 0.f, nullptr, p->y + b0));
     if (rest > 0)
-      gemv_n_kernel<<<(rest + GR - 1) / GR, kThreads, kGemvSmem, s>>>(p->W + (b0 + bI) + (long long)b0 * ldw, ldw, rest,
-                                                             bI, p->y + b0, -1.f, 1.f, p->t + b0 + bI,
-                                                             p->t + b0 + bI, ld);
+      CUCHOL_CHECK_CU(gemv(false, p->W + (b0 + bI) + (long long)b0 * ldw, ldw, rest, bI, p->y + b0, -1.f, 1.f,
+                           p->t + b0 + bI, p->t + b0 + bI));
   }
   for (int I = nT - 1; I >= 0; --I) {
     const int b0 = I * NBT, bI = std::min(NBT, n - b0);
     const float* D = p->Dinv + (size_t)I * NBT * NBT;
-    gemv_t_kernel<<<(bI + GR - 1) / GR, kThreads, kGemvSmem, s>>>(D, NBT, bI, bI, p->y + b0, 1.f, 0.f, nullptr,
-                                                         p->zf + b0, ld);
-    if (b0 > 0)
-      gemv_t_kernel<<<(b0 + GR - 1) / GR, kThreads, kGemvSmem, s>>>(p->W + b0, ldw, b0, bI, p->zf + b0, -1.f, 1.f, p->y,
-                                                           p->y, ld);
+    CUCHOL_CHECK_CU(gemv(true, D, NBT, bI, bI, p->y + b0, 1.f, 0.f, nullptr, p->zf + b0));
+    if (b0 > 0) CUCHOL_CHECK_CU(gemv(true, p->W + b0, ldw, b0, bI, p->zf + b0, -1.f, 1.f, p->y, p->y));
   }
   scale_out_kernel<<<vb, 256, 0, s>>>(p->zf, p->s, n, ld, Z);
   CUCHOL_CHECK(cudaGetLastError());
-  p->h->launches += 2 + 4 * nT;
+  p->h->launches += 2;
   return CUDA_SUCCESS;
 }
 
@@ -1162,6 +1205,7 @@ void free_mixed(CUcholMixed p) {
   cudaFree(p->s);
   cudaFree(p->Dinv);
   cudaFree(p->dtmp);
+  cudaFree(p->gpart);
   cudaFree(p->x);
   cudaFree(p->t);
   cudaFree(p->U);
@@ -1319,6 +1363,9 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
   const int nT = (n + NBT - 1) / NBT;
   if ((e = cudaMalloc(&p->Dinv, sizeof(float) * (size_t)nT * NBT * NBT)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&p->dtmp, sizeof(float) * (size_t)n * NBT / 4 + 256)) != cudaSuccess) return fail(e);
+  // split k only when a GEMV has fewer than 2 * SMs row blocks: at most NBT / 256 splits
+  const size_t gpart = (size_t)(NBT / 256) * (2 * h->num_sms + 1) * GR * NR;
+  if ((e = cudaMalloc(&p->gpart, sizeof(float) * gpart)) != cudaSuccess) return fail(e);
   // x r z p q b in one block, then the reduction scratch
   if ((e = cudaMalloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
   p->r = p->x + p->ld * NR;
