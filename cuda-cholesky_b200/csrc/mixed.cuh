@@ -7,7 +7,8 @@
 // Factor (cuDcholMixedCreate):
 //   1. s_i = 1 / sqrt(a_ii); W = S A S + shift * I in FP32 (lower, our own buffer):
 //      the symmetric diagonal scaling removes the row/column scaling part of
-//      kappa(A) before any rounding to low precision.
+//      kappa(A) before any rounding to low precision.  The shift starts at u / 16 (u
+//      the operand unit roundoff) and grows 8x after a breakdown.
 //   2. Right-looking blocked Cholesky of W with the two-stream schedule of ?potrf
 //      (outer blocks of 512 columns = four 128-column sub-panels, lookahead 1):
 //        - diagonal blocks in FP64 (the ?potrf diagonal kernel on an FP64 copy),
@@ -1298,7 +1299,7 @@ CUresult mixed_refactor(CUcholMixed p, long* info) {
   // factor S A S + shift I; on a breakdown retry with 8x the shift (automatic mode)
   const double u = (sizeof(Op) == 2) ? 0x1p-8 : 0x1p-11;
   const double shift_in = p->shift_request;
-  double shift = shift_in >= 0.0 ? shift_in : u;
+  double shift = shift_in >= 0.0 ? shift_in : u / 16;
   long finfo = 0;
   const int nT = (n + NBT - 1) / NBT;
   for (int attempt = 0; attempt < (shift_in >= 0.0 ? 1 : 4); ++attempt, shift *= 8.0) {

@@ -91,8 +91,9 @@ CUresult cuSpotrs(CULAPACKhandle, CBlasUplo, size_t, size_t, CUdeviceptr, size_t
  *   |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf) <= tol.
  *   cuDcholMixedCreate  scale, factor; keeps the pointer A (read by every solve, so
  *                       leave it unchanged while the plan lives).  shift < 0 picks
- *                       the shift automatically (u, 8u, 64u, 512u with u the
- *                       operand unit roundoff, until the factor succeeds).
+ *                       the shift automatically (u/16, u/2, 4u, 32u with u the
+ *                       operand unit roundoff 2^-8 or 2^-11, until the factor
+ *                       succeeds).
  *                       *info > 0: A has a non-positive diagonal entry at that row,
  *                       or the low-precision factor broke down at that column.
  *   cuDcholMixedSolve   X := A^-1 B (n x nrhs, FP64), tol <= 0 -> sqrt(n) eps,
