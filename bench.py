@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--syrk", nargs=2, type=int, metavar=("M", "K"),
                     help="only the dominant kernel: two cuDsyrk(L, N) launches of order M, rank K "
                          "(warm-up + measured), for profiling")
+    ap.add_argument("--syrk-lowp", nargs=3, metavar=("M", "K", "PREC"),
+                    help="only the mixed factor's trailing update: two cuSsyrkLowp launches of order M, "
+                         "rank K, PREC bf16 or tf32 (warm-up + measured), for profiling")
     return ap.parse_args()
 
 
@@ -81,6 +84,29 @@ def run_syrk_only(m: int, k: int) -> None:
         print(json.dumps({"kernel": "cuDsyrk L,N", "m": m, "k": k, "rc": rc, "ms": ms,
                           "tflops": float(m) * (m + 1) * k / (ms / 1e3) / 1e12}), flush=True)
     bh.close()
+
+
+def run_syrk_lowp_only(m: int, k: int, prec: str) -> None:
+    import torch
+    import cucholesky as cc
+    dev = torch.device("cuda", 0)
+    h = cc.Handle()
+    p = cc.MIXED_BF16 if prec == "bf16" else cc.MIXED_TF32
+    Q = (torch.rand((m, k), device=dev, dtype=torch.float32) * 2 - 1).to(
+        torch.bfloat16 if prec == "bf16" else torch.float32)
+    C = torch.zeros((m, m), device=dev, dtype=torch.float32)
+    for _ in range(2):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = cc.call_syrk_lowp(h, p, m, k, -1.0, Q.data_ptr(), k, C.data_ptr(), m)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(json.dumps({"kernel": f"cuSsyrkLowp {prec}", "m": m, "k": k, "rc": rc, "ms": ms,
+                          "tflops": float(m) * (m + 1) * k / (ms / 1e3) / 1e12,
+                          "c_gbs": float(m) * (m + 1) / 2 * 8 / (ms / 1e3) / 1e9}), flush=True)
+    h.close()
 
 
 def dist_env():
@@ -426,6 +452,37 @@ def run_mixed(args) -> None:
             del X
         del A, B
         torch.cuda.empty_cache()
+    # roofline of the dominant factor kernel: the tcgen05 trailing update at its largest
+    # launch of this factorisation (m = n - 512 rows, k = 512), timed alone with CUDA events
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    tf32_peak = bf16_peak / 2          # dense TF32 rate is half the BF16 rate on these tensor cores
+    m, kq = n - 512, 512
+    Cm = torch.rand((m, m), device=dev, dtype=torch.float32)
+    upd = {}
+    for prec, pname, qdt in ((cc.MIXED_TF32, "tf32", torch.float32), (cc.MIXED_BF16, "bf16", torch.bfloat16)):
+        Qm = (torch.rand((m, kq), device=dev, dtype=torch.float32) * 2 - 1).to(qdt)
+        for _ in range(3):
+            cc.call_syrk_lowp(h, prec, m, kq, -1.0, Qm.data_ptr(), kq, Cm.data_ptr(), m)
+        ts = []
+        for _ in range(5):
+            ms, _ = timed(lambda: cc.call_syrk_lowp(h, prec, m, kq, -1.0, Qm.data_ptr(), kq, Cm.data_ptr(), m))
+            ts.append(ms)
+        t = statistics.median(ts) / 1e3
+        flop = float(m) * (m + 1) * kq          # lower triangle, 2 flop per multiply-add
+        cbytes = float(m) * (m + 1) / 2 * 8     # C read + written once (FP32)
+        upd[pname] = {"ms": t * 1e3, "tflops": flop / t / 1e12,
+                      "tensor_frac": flop / t / 1e12 / (tf32_peak if pname == "tf32" else bf16_peak),
+                      "c_gbs": cbytes / t / 1e9}
+        del Qm
+    del Cm
+    torch.cuda.empty_cache()
     ok = [c for c in cases if c["k"] <= 2.0 and c["precision"] == "tf32"]
     value = min(c["speedup"] for c in ok) if ok else None
     line = {
@@ -437,6 +494,12 @@ def run_mixed(args) -> None:
                                "16 rhs ~ N(0,1), lower", "n": n, "nrhs": nrhs, "k": ks,
                    "value": "min over k <= 2 (kappa <= ~4e7) of the TF32 speedup"},
         "cases": cases,
+        "roofline": {"bound": "hbm", "achieved": upd["tf32"]["c_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                     "frac": upd["tf32"]["c_gbs"] / hbm_peak, "traffic": None,
+                     "kernel": f"tc::update_kernel<tf32> (cuSsyrkLowp) m={m} k={kq}: C read+write, FP32",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                     "tensor_tflops": upd["tf32"]["tflops"], "tensor_frac_of_tf32": upd["tf32"]["tensor_frac"],
+                     "tf32_peak_tflops": tf32_peak, "bf16": upd["bf16"], "bf16_peak_tflops": bf16_peak},
     }
     print(json.dumps(line), flush=True)
     h.close()
@@ -447,6 +510,9 @@ def main():
     rank, world, local = dist_env()
     if args.syrk:
         run_syrk_only(*args.syrk)
+        return
+    if args.syrk_lowp:
+        run_syrk_lowp_only(int(args.syrk_lowp[0]), int(args.syrk_lowp[1]), args.syrk_lowp[2])
         return
     if args.workload == "batched":
         if rank == 0:

@@ -1067,11 +1067,12 @@ CUresult precond(CUcholMixed p, const double* R, double* Z, cudaStream_t s) {
   return CUDA_SUCCESS;
 }
 
-// C := C - Q(a0 + i) Q(b0 + j)^T on the lower tiles of an m x ncols FP32 region whose
+// C := C + alpha Q(a0 + i) Q(b0 + j)^T (alpha = -1 in the factor) on the lower tiles of an
+// m x ncols FP32 region whose
 // top-left element is on the diagonal; Q k-major (q_rows x k used, row pitch ldq).
 template <typename Op>
 CUresult tc_update(CULAPACKhandle h, const Op* q, long long ldq, int q_rows, int k, int a0, int b0, float* c,
-                   long long ldc, int m, int ncols, cudaStream_t s, const int* stop) {
+                   long long ldc, int m, int ncols, cudaStream_t s, const int* stop, float alpha = -1.f) {
   if (m <= 0 || ncols <= 0 || k <= 0) return CUDA_SUCCESS;
   EncodeTiledFn fn = encode_tiled();
   if (fn == nullptr) return CUDA_ERROR_NOT_SUPPORTED;
@@ -1102,7 +1103,7 @@ CUresult tc_update(CULAPACKhandle h, const Op* q, long long ldq, int q_rows, int
   prm.k = k;
   prm.a_row0 = a0;
   prm.b_row0 = b0;
-  prm.alpha = -1.f;
+  prm.alpha = alpha;
   prm.lower_only = 1;
   prm.tiles_m = (m + tc::BM - 1) / tc::BM;
   prm.tiles_n = (ncols + tc::BN - 1) / tc::BN;
@@ -1565,6 +1566,36 @@ extern "C" CUCHOL_EXPORT CUresult cuDcholMixedCreate(CUcholMixed* plan, CULAPACK
   if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
   if (precision == CUCHOL_MIXED_BF16) return mx::mixed_create<__nv_bfloat16>(plan, h, uplo, n, A, lda, shift, info);
   return mx::mixed_create<float>(plan, h, uplo, n, A, lda, shift, info);
+}
+
+// The factor's trailing-update kernel on its own: C(i, j) += alpha sum_l Q(i, l) Q(j, l)
+// for i >= j, Q k-major (row i at Q + i * ldq) in BF16 or TF32 (FP32 words), C FP32
+// column-major.  Queued on `stream`.
+extern "C" CUCHOL_EXPORT CUresult cuSsyrkLowp(CULAPACKhandle h, int precision, size_t n, size_t k, float alpha,
+                                              CUdeviceptr Q, size_t ldq, CUdeviceptr C, size_t ldc,
+                                              CUstream stream) {
+  long info = 0;
+  const size_t esize = (precision == CUCHOL_MIXED_BF16) ? 2 : 4;
+  if (precision != CUCHOL_MIXED_BF16 && precision != CUCHOL_MIXED_TF32) info = 2;
+  else if (n > (size_t)INT_MAX) info = 3;
+  else if (k > (size_t)INT_MAX) info = 4;
+  else if (ldq < k || (ldq * esize) % 16 != 0 || (Q & 15) != 0) info = 7;
+  else if (ldc < n || ldc % 4 != 0 || (C & 15) != 0) info = 9;
+  if (info != 0) {
+    if (xerbla != nullptr) xerbla("cuSsyrkLowp", info);
+    return CUDA_ERROR_INVALID_VALUE;
+  }
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0 || k == 0) return CUDA_SUCCESS;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int* stop = h->d_words + 5;   // never set: the update has no earlier step to depend on
+  CUCHOL_CHECK(cudaMemsetAsync(stop, 0, sizeof(int), s));
+  if (precision == CUCHOL_MIXED_BF16)
+    return mx::tc_update<__nv_bfloat16>(h, reinterpret_cast<const __nv_bfloat16*>(Q), (long long)ldq, (int)n,
+                                        (int)k, 0, 0, reinterpret_cast<float*>(C), (long long)ldc, (int)n, (int)n, s,
+                                        stop, alpha);
+  return mx::tc_update<float>(h, reinterpret_cast<const float*>(Q), (long long)ldq, (int)n, (int)k, 0, 0,
+                              reinterpret_cast<float*>(C), (long long)ldc, (int)n, (int)n, s, stop, alpha);
 }
 
 extern "C" CUCHOL_EXPORT CUresult cuDcholMixedRefactor(CUcholMixed p, long* info) {

@@ -82,7 +82,7 @@ def extension_symbols() -> list[str]:
     names += ["cuLAPACKGetLaunchCount", "cuDcholBatchedCreate", "cuScholBatchedCreate", "cuCholBatchedRun",
               "cuCholBatchedResults", "cuCholBatchedGetBlockSize", "cuCholBatchedDestroy", "cuDlogdetNoAlloc",
               "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
-              "cuCholMixedGetFactor",
+              "cuCholMixedGetFactor", "cuSsyrkLowp",
               "cuCholMixedDestroy", "cuDposvMixed"]
     return names
 
@@ -459,6 +459,16 @@ class MixedPlan:
             self.close()
         except Exception:
             pass
+
+
+def call_syrk_lowp(h: Handle, precision: int, n: int, k: int, alpha: float, q: int, ldq: int, c: int,
+                   ldc: int, stream: int = 0) -> int:
+    """cuSsyrkLowp: C(lower) += alpha Q Q^T with BF16 / TF32 Q (k-major) and FP32 C."""
+    L = lib()
+    L.cuSsyrkLowp.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_float, C.c_uint64, C.c_size_t,
+                              C.c_uint64, C.c_size_t, C.c_void_p]
+    L.cuSsyrkLowp.restype = C.c_int
+    return L.cuSsyrkLowp(h.value, precision, n, k, alpha, q, ldq, c, ldc, C.c_void_p(stream))
 
 
 def call_posv_mixed(h: Handle, uplo: str, n: int, nrhs: int, a: int, lda: int, b: int, ldb: int, x: int,

@@ -120,6 +120,15 @@ CUresult cuCholMixedGetFactor(CUcholMixed, CUdeviceptr *, size_t *, CUdeviceptr 
 CUresult cuCholMixedDestroy(CUcholMixed);
 CUresult cuDposvMixed(CULAPACKhandle, CBlasUplo, size_t, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t,
                       CUdeviceptr, size_t, int, int *, double *, long *);
+/* The mixed factor's trailing-update kernel on its own (tcgen05 tensor cores):
+ *   C(i, j) += alpha * sum_l Q(i, l) Q(j, l)   for i >= j (lower triangle of C only)
+ * with Q an n x k matrix stored k-major (row i at Q + i*ldq elements) in BF16
+ * (CUCHOL_MIXED_BF16) or in FP32 words read as TF32 (CUCHOL_MIXED_TF32), C FP32
+ * column-major, FP32 accumulation; queued on `stream`.  Q and C 16-byte aligned,
+ * ldq * element size and ldc * 4 multiples of 16 bytes (else XERBLA with the position
+ * and CUDA_ERROR_INVALID_VALUE). */
+CUresult cuSsyrkLowp(CULAPACKhandle, int, size_t, size_t, float, CUdeviceptr, size_t, CUdeviceptr, size_t,
+                     CUstream);
 #ifdef __cplusplus
 }
 #endif

@@ -86,3 +86,47 @@ def test_binding_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(cucholesky, "_lib", None)
     with pytest.raises(FileNotFoundError):
         cucholesky.lib()
+
+
+def test_extension_argument_errors():
+    """Argument checks of the additions run before any device work: XERBLA gets the
+    position and CUDA_ERROR_INVALID_VALUE comes back (no handle needed)."""
+    lib = cucholesky.lib()
+    calls = []
+    XERBLA = C.CFUNCTYPE(None, C.c_char_p, C.c_long)
+
+    def hook(name, info):
+        calls.append((name.decode(), info))
+
+    cb = XERBLA(hook)
+    xer = C.c_void_p.in_dll(lib, "xerbla")
+    old = xer.value
+    xer.value = C.cast(cb, C.c_void_p).value
+    try:
+        f = lib.cuDpotrs
+        f.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t,
+                      C.POINTER(C.c_long)]
+        info = C.c_long(0)
+        assert f(None, ord("L"), 10, 1, 0, 10, 0, 5, C.byref(info)) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert info.value == -8 and calls[-1] == ("cuDpotrs", 8)
+        g = lib.cuDcholMixedCreate
+        g.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.c_int,
+                      C.c_double, C.POINTER(C.c_long)]
+        plan = C.c_void_p()
+        assert g(C.byref(plan), None, ord("L"), 10, 0, 10, 3, -1.0, C.byref(info)) == \
+            cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert info.value == -7 and calls[-1] == ("cuDcholMixedCreate", 7)
+        assert g(C.byref(plan), None, ord("L"), 10, 0, 9, 1, -1.0, C.byref(info)) == \
+            cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert info.value == -6
+        k = lib.cuSsyrkLowp
+        k.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t, C.c_float, C.c_uint64, C.c_size_t, C.c_uint64,
+                      C.c_size_t, C.c_void_p]
+        assert k(None, 1, 16, 16, -1.0, 0, 12, 0, 16, None) == cucholesky.CUDA_ERROR_INVALID_VALUE   # 24 bytes
+        assert calls[-1] == ("cuSsyrkLowp", 7)
+        assert k(None, 2, 16, 16, -1.0, 0, 16, 0, 18, None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert calls[-1] == ("cuSsyrkLowp", 9)
+        assert k(None, 5, 16, 16, -1.0, 0, 16, 0, 16, None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert calls[-1] == ("cuSsyrkLowp", 2)
+    finally:
+        xer.value = old

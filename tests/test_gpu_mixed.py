@@ -172,3 +172,38 @@ def test_posv_mixed_not_spd_falls_back(handle):
     torch.cuda.synchronize()
     assert rc == 0 and it == -3
     assert info == info_ref == 101
+
+
+@pytest.mark.parametrize("prec", [cc.MIXED_BF16, cc.MIXED_TF32])
+@pytest.mark.parametrize("n,k", [(1, 8), (127, 64), (300, 200), (1024, 512)])
+def test_syrk_lowp(handle, prec, n, k):
+    """cuSsyrkLowp (the tcgen05 trailing-update kernel) against an FP64 product of
+    the same rounded operands: lower triangle updated, upper triangle untouched."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(n * 7 + k)
+    ldq = (k + 7) // 8 * 8 if prec == cc.MIXED_BF16 else (k + 3) // 4 * 4
+    Q32 = torch.rand((n, ldq), generator=g, device="cuda", dtype=torch.float32) * 2 - 1
+    if prec == cc.MIXED_BF16:
+        Q = Q32.to(torch.bfloat16)
+        Qd = Q.double()[:, :k]
+    else:
+        # TF32 operands: values already representable, so rounding mode does not matter
+        Q = (Q32.view(torch.int32) & ~0x1FFF).view(torch.float32)
+        Qd = Q.double()[:, :k]
+    ldc = (n + 3) // 4 * 4
+    Cm = torch.rand((n, ldc), generator=g, device="cuda", dtype=torch.float32)   # column j = row j of Cm
+    C0 = Cm.clone()
+    rc = cc.call_syrk_lowp(handle, prec, n, k, -1.0, Q.data_ptr(), ldq, Cm.data_ptr(), ldc)
+    torch.cuda.synchronize()
+    assert rc == 0
+    ref = C0.double()[:, :n].T - Qd @ Qd.T        # column-major C as a (n, n) matrix
+    got = Cm.double()[:, :n].T
+    low = torch.tril(torch.ones(n, n, dtype=torch.bool, device="cuda"))
+    # FP32 accumulation of k exact products, then one FP32 add to C:
+    # |err| <= gamma_{k+1} (|Q||Q|^T + |C|), gamma_j = j u / (1 - j u), u = 2^-24
+    u = 2.0 ** -24
+    gamma = (k + 1) * u / (1 - (k + 1) * u)
+    bound = gamma * (Qd.abs() @ Qd.abs().T + C0.double()[:, :n].T.abs())
+    assert bool(((got - ref).abs() <= bound)[low].all()), ((got - ref).abs() - bound)[low].max().item()
+    assert torch.equal(got[~low], C0.double()[:, :n].T[~low])
