@@ -938,3 +938,4 @@ CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 
 #include "batched.cuh"
 #include "mixed.cuh"
+#include "ozaki_driver.cuh"

@@ -82,7 +82,7 @@ def extension_symbols() -> list[str]:
     names += ["cuLAPACKGetLaunchCount", "cuDcholBatchedCreate", "cuScholBatchedCreate", "cuCholBatchedRun",
               "cuCholBatchedResults", "cuCholBatchedGetBlockSize", "cuCholBatchedDestroy", "cuDlogdetNoAlloc",
               "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
-              "cuCholMixedGetFactor", "cuSsyrkLowp",
+              "cuCholMixedGetFactor", "cuSsyrkLowp", "cuDpotrfOzaki",
               "cuCholMixedDestroy", "cuDposvMixed"]
     return names
 

@@ -128,5 +128,11 @@ def test_extension_argument_errors():
         assert calls[-1] == ("cuSsyrkLowp", 9)
         assert k(None, 5, 16, 16, -1.0, 0, 16, 0, 16, None) == cucholesky.CUDA_ERROR_INVALID_VALUE
         assert calls[-1] == ("cuSsyrkLowp", 2)
+        z = lib.cuDpotrfOzaki
+        z.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.c_int, C.POINTER(C.c_long)]
+        assert z(None, ord("L"), 10, 0, 10, 9, C.byref(info)) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert info.value == -6 and calls[-1] == ("cuDpotrfOzaki", 6)
+        assert z(None, ord("L"), 10, 0, 5, 8, C.byref(info)) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert info.value == -5
     finally:
         xer.value = old
