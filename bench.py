@@ -45,14 +45,15 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--n", type=int, default=None,
+                    help="matrix order (default: 16384 for potrf, 32768 for mixed, 65536 for ozaki)")
     ap.add_argument("--uplo", default="L")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--kappa", default="0,1,2,3",
                     help="mixed workload: exponents k of D = diag(10^(k i/(n-1))), comma separated")
-    ap.add_argument("--workload", default="potrf", choices=["potrf", "batched", "mixed"],
+    ap.add_argument("--workload", default="potrf", choices=["potrf", "batched", "mixed", "ozaki"],
                     help="potrf: FP64 dpotrf n=16384 (default line); batched: 10,000 uneven SPD "
                          "kernel matrices, potrf + logdet + potri in one graph launch")
     ap.add_argument("--dtype", default="d", choices=["d", "s"], help="batched workload precision")
@@ -377,7 +378,7 @@ def run_mixed(args) -> None:
     import cucholesky as cc
     from cucholesky import matgen
     dev = torch.device("cuda", 0)
-    n = args.n if args.n != N_DEFAULT else 32768
+    n = args.n if args.n is not None else 32768
     nrhs = 16
     ks = [float(k) for k in args.kappa.split(",")]
     h = cc.Handle()
@@ -505,8 +506,118 @@ def run_mixed(args) -> None:
     h.close()
 
 
+def run_ozaki(args) -> None:
+    """Large split-precision factor: dpotrf + dpotri of one FP64 SPD matrix
+    A = G G^T / n + I (G uniform[-1, 1], seed 0), n = 65536 (34 GB) by default, with the
+    trailing updates on the FP64 DMMA engine (cuDpotrf) and as the Ozaki-sliced INT8
+    emulation (cuDpotrfOzaki, 8 slices); the inverse (cuDpotri, the same native path
+    for both) follows the Ozaki factor.  Errors are estimated with 4 Gaussian probes X
+    (||E X||_F^2 / 4 estimates ||E||_F^2, O(n^2) work): the backward error
+    ||A - L L^T||_F / (n eps ||A||_F) of each factor, and the inverse residual
+    ||X - A (inv(A) X)||_F / (n eps ||A||_F ||inv(A) X||_F)."""
+    import ctypes as C
+    import torch
+    import cucholesky as cc
+    dev = torch.device("cuda", 0)
+    n = args.n if args.n is not None else 65536
+    eps = 2.0 ** -52
+    h = cc.Handle()
+    L = cc.lib()
+    L.cuDpotrfOzaki.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_size_t, C.c_int,
+                                C.POINTER(C.c_long)]
+    L.cuDpotrfOzaki.restype = C.c_int
+
+    def ozaki(ptr, nn, ld):
+        info = C.c_long(0)
+        rc = L.cuDpotrfOzaki(h.value, ord("L"), nn, ptr, ld, 8, C.byref(info))
+        return rc, info.value
+
+    # warm-up of both paths on a small matrix (kernel loading), untimed
+    w = make_spd_device(torch, 2048, 1, dev)
+    for f in (lambda t: cc.call_potrf(h, "D", "L", 2048, t.data_ptr(), 2048), lambda t: ozaki(t.data_ptr(), 2048, 2048)):
+        t = w.clone()
+        f(t)
+    del w, t
+    A0 = make_spd_device(torch, n, 0, dev)        # symmetric: row- and column-major agree
+    anorm = torch.linalg.norm(A0).item()
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    X = torch.randn((n, 4), generator=g, device=dev, dtype=torch.float64)
+
+    def factor_error(T):
+        # T: (n, n) tensor whose transpose is the column-major factor (L in its lower part)
+        # L (L^T X) in row chunks of T = L^T (upper part of T): V = triu(T) X, W = triu(T)^T V
+        V = torch.empty_like(X)
+        ch = 4096
+        for a in range(0, n, ch):
+            b = min(n, a + ch)
+            blk = torch.triu(T[a:b, a:], diagonal=0)
+            V[a:b] = blk @ X[a:]
+            del blk
+        W = torch.zeros_like(X)
+        for a in range(0, n, ch):
+            b = min(n, a + ch)
+            blk = torch.triu(T[a:b, a:], diagonal=0)
+            W[a:] += blk.T @ V[a:b]
+            del blk
+        E = A0 @ X - W
+        return float(torch.linalg.norm(E).item() / 2.0 / (n * eps * anorm))   # / sqrt(4 probes)
+
+    Aw = torch.empty_like(A0)
+    out = {}
+    for name, call in (("native_dmma", lambda: cc.call_potrf(h, "D", "L", n, Aw.data_ptr(), n)),
+                       ("ozaki_int8_8slices", lambda: ozaki(Aw.data_ptr(), n, n))):
+        Aw.copy_(A0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc, info = call()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"potrf_ms": ms, "tflops": n ** 3 / 3 / (ms / 1e3) / 1e12, "rc": rc, "info": info,
+                     "backward_error_n_eps_probe": factor_error(Aw)}
+    # the inverse from the Ozaki factor (native ?potri)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rc, info = cc.call_potri(h, "D", "L", n, Aw.data_ptr(), n)
+    e1.record()
+    torch.cuda.synchronize()
+    potri_ms = e0.elapsed_time(e1)
+    # inverse residual: Y = inv(A) X from the lower triangle of Aw (symmetric), R = X - A Y
+    ch = 4096
+    Y = torch.zeros_like(X)
+    for a in range(0, n, ch):
+        b = min(n, a + ch)
+        blk = torch.triu(Aw[a:b, a:], diagonal=0)   # rows a..b of the upper part of T = lower columns of inv(A)
+        Y[a:b] += blk @ X[a:]
+        strict = torch.triu(Aw[a:b, a:], diagonal=1)
+        Y[a:] += strict.T @ X[a:b]
+        del blk, strict
+    R = X - A0 @ Y
+    ynorm = torch.linalg.norm(Y).item()
+    inv_res = float(torch.linalg.norm(R).item() / (anorm * ynorm * n * eps))
+    line = {
+        "metric": "ozaki_sliced_dpotrf_speedup_vs_native_dmma", "value": out["native_dmma"]["potrf_ms"] /
+        out["ozaki_int8_8slices"]["potrf_ms"], "unit": "x", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": out["ozaki_int8_8slices"]["potrf_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (int8 slices)", "data": "synthetic",
+        "config": {"workload": f"dpotrf + dpotri L FP64 n={n}, A=G*G^T/n+I, G~U[-1,1]", "n": n, "slices": 8},
+        "arms": out, "potri_ms_after_ozaki": potri_ms, "potri_rc_info": [rc, info],
+        "inverse_residual_probe_n_eps": inv_res,
+        "error_note": "4 Gaussian probes: ||A X - L L^T X||_F / (2 n eps ||A||_F); ||X - A inv(A) X||_F / "
+                      "(n eps ||A||_F ||inv(A) X||_F)",
+    }
+    print(json.dumps(line), flush=True)
+    h.close()
+
+
 def main():
     args = parse()
+    if args.n is None and args.workload in ("potrf", "batched"):
+        args.n = N_DEFAULT
     rank, world, local = dist_env()
     if args.syrk:
         run_syrk_only(*args.syrk)
@@ -521,6 +632,10 @@ def main():
     if args.workload == "mixed":
         if rank == 0:
             run_mixed(args)
+        return
+    if args.workload == "ozaki":
+        if rank == 0:
+            run_ozaki(args)
         return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
