@@ -133,9 +133,9 @@ CUresult cuSsyrkLowp(CULAPACKhandle, int, size_t, size_t, float, CUdeviceptr, si
 /* FP64 Cholesky factor (cuDpotrf contract: in place, info of the first failing
  * leading minor) whose trailing updates run as an Ozaki-sliced emulation on the INT8
  * tensor cores: every panel row is scaled by a power of two and cut into `slices`
- * signed 8-bit slices (4..8, 0 = 8), the slice products are exact INT32 sums, and
- * only the final FP64 combination rounds (8 slices: FP64-level accuracy).  No
- * counterpart in the reference library. */
+ * signed 8-bit slices (4..8; 0 = 8 below n = 8192, 7 from there on), the slice
+ * products are exact INT32 sums, and only the final FP64 combination rounds (7 or 8
+ * slices: FP64-level backward error).  No counterpart in the reference library. */
 CUresult cuDpotrfOzaki(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, int, long *);
 #ifdef __cplusplus
 }

@@ -85,3 +85,12 @@ def test_ozaki_fewer_slices(handle):
     assert info == 0
     b8, b4 = _berr(A, F8, "L"), _berr(A, F4, "L")
     assert b8 <= 10 < b4 < 1e10          # 4 slices: ~28-bit products, still a factor
+
+
+def test_ozaki_seven_slices(handle):
+    """7 slices (the default from n = 8192 on) still meet the FP64 bound at n = 4096."""
+    n = 4096
+    A = matgen.spd("d", n, seed=21)
+    F7, info = _ozaki(handle, "L", A, 7)
+    assert info == 0
+    assert _berr(A, F7, "L") <= 10
