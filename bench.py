@@ -264,21 +264,37 @@ def run_batched(args) -> None:
     import numpy as np
     import torch
     import cucholesky as cc
-    dev = torch.device("cuda", 0)
+    from cucholesky import shard
+    rank, world, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    pg = None
+    if world > 1:
+        # the batch shards by matrix (cost-balanced), no exchange in the data path
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+        pg = dist
     p = args.dtype
     tdt = torch.float64 if p == "d" else torch.float32
     B = 10000
     rng = np.random.default_rng(0)
-    sizes = rng.integers(8, 513, B).tolist()
+    sizes_all = rng.integers(8, 513, B).tolist()
+    mine = shard.partition_by_cost(sizes_all, world)[rank] if world > 1 else list(range(B))
+    sizes = [sizes_all[i] for i in mine]
     off, t = [], 0
     for n in sizes:
         off.append(t)
         t += n * n
-    buf0 = torch.empty(t, dtype=tdt, device=dev)
+    buf0 = torch.empty(max(t, 1), dtype=tdt, device=dev)
     g = torch.Generator(device=dev)
     g.manual_seed(0)
-    for n, o in zip(sizes, off):
+    pos = {b: q for q, b in enumerate(mine)}
+    for b, n in enumerate(sizes_all):          # every rank draws the same points in order
         x = torch.rand(n, 3, dtype=torch.float64, device=dev, generator=g)
+        if b not in pos:
+            continue
+        o = off[pos[b]]
         K = torch.exp(-torch.cdist(x, x).pow(2) / (2 * 0.3 ** 2)) + 1e-4 * torch.eye(n, dtype=torch.float64, device=dev)
         buf0[o:o + n * n] = K.to(tdt).reshape(-1)     # symmetric: row- and column-major agree
     buf = buf0.clone()
@@ -286,7 +302,7 @@ def run_batched(args) -> None:
     t0 = time.perf_counter()
     plan = cc.BatchedPlan(h, buf, sizes, off, flags=7, nb=0)
     plan_s = time.perf_counter() - t0
-    flops = float(sum(n ** 3 for n in sizes))        # n^3/3 (potrf) + 2n^3/3 (potri)
+    flops = float(sum(n ** 3 for n in sizes_all))    # n^3/3 (potrf) + 2n^3/3 (potri), whole batch
     for _ in range(args.warmup):
         buf.copy_(buf0)
         plan.run()
@@ -294,17 +310,37 @@ def run_batched(args) -> None:
     times = []
     for _ in range(args.steps):
         buf.copy_(buf0)
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         plan.run()
         e1.record()
         torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+        ms_r = e0.elapsed_time(e1)
+        if pg is not None:                           # the step time is the slowest rank's
+            tms = torch.tensor([ms_r], dtype=torch.float64, device=dev)
+            pg.all_reduce(tms, op=pg.ReduceOp.MAX)
+            ms_r = float(tms.item())
+        times.append(ms_r)
     info, ld = plan.results()
+    if pg is not None:                               # the one collective: gather the results
+        info_all, ld_all = shard.gather_results(mine, info, ld, B, device=dev)
+        n_failed = int((info_all != 0).sum().item())
+    else:
+        n_failed = sum(1 for i in info if i != 0)
     ms = statistics.mean(times)
+    if rank != 0:
+        plan.close()
+        h.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    B_local = len(sizes)
     # accuracy on a sample: inverse residual and log det against FP64 numpy
-    chk = rng.choice(B, 20, replace=False)
+    chk = rng.choice(B_local, min(20, B_local), replace=False)
     host = buf.cpu().numpy()
     hres = buf0.cpu().numpy()
     worst_res = worst_ld = 0.0
@@ -319,7 +355,7 @@ def run_batched(args) -> None:
         ref = float(np.linalg.slogdet(A)[1])
         worst_ld = max(worst_ld, float(abs(ld[b] - ref) / (n * float(eps) * max(1.0, abs(ref)))))
     # the same work as a loop of plain per-matrix calls, on a sample
-    sample = rng.choice(B, 200, replace=False)
+    sample = rng.choice(B_local, min(200, B_local), replace=False)
     P = p.upper()
     # untimed warm-up of the plain calls (first launches load their kernels)
     for b in sample[:8]:
@@ -349,21 +385,25 @@ def run_batched(args) -> None:
     loop_total_ms = loop_ms / frac
     line = {
         "metric": "batched_potrf_logdet_potri_matrices_per_s", "value": B / (ms / 1e3), "unit": "matrices/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if p == "d" else "f32", "data": "synthetic",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64" if p == "d" else "f32",
+        "data": "synthetic",
         "config": {"workload": "10,000 squared-exponential kernel matrices, n_i ~ U{8..512}, lower",
-                   "batch": B, "sum_n3": flops, "graph_launches_per_step": 1, "nb": plan.nb},
+                   "batch": B, "sum_n3": flops, "graph_launches_per_step": 1, "nb": plan.nb,
+                   "parallelism": f"sharded by cost over {world} GPUs" if world > 1 else "single"},
         "gflops": flops / (ms / 1e3) / 1e9,
         "loop_of_plain_calls_ms_extrapolated": loop_total_ms,
         "speedup_vs_loop": loop_total_ms / ms,
         "loop_sample": "200 matrices (seeded), cu?potrf + cu?logdet + cu?potri each, extrapolated by sum n^3",
-        "failed_matrices": sum(1 for i in info if i != 0),
+        "failed_matrices": n_failed,
         "worst_inverse_residual_sampled": worst_res, "worst_logdet_rel_err_n_eps_sampled": worst_ld,
         "plan_build_s": plan_s,
     }
     print(json.dumps(line), flush=True)
     plan.close()
     h.close()
+    if pg is not None:
+        pg.destroy_process_group()
 
 
 def run_mixed(args) -> None:
