@@ -936,6 +936,7 @@ CUCHOL_API_RANKK(cuDsyrk, double, false)
 CUCHOL_API_RANKK(cuCherk, cuFloatComplex, true)
 CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 
+#include "blas3.cuh"
 #include "batched.cuh"
 #include "mixed.cuh"
 #include "ozaki_driver.cuh"

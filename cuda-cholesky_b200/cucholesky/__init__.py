@@ -72,7 +72,8 @@ def exported_symbols() -> list[str]:
     names = ["cuLAPACKCreate", "cuLAPACKDestroy", "xerbla", "errorHandler", "cuBLASCreate", "cuBLASDestroy",
              "cuSsyrk", "cuDsyrk", "cuCherk", "cuZherk"]
     for p in "SDCZ":
-        names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet", "gemm2")]
+        names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet", "gemm2", "trsm",
+                                         "trmm2")]
     return names
 
 
@@ -244,6 +245,16 @@ def _declare_blas(L: C.CDLL) -> None:
         f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_size_t, S, C.c_uint64, C.c_size_t,
                       C.c_uint64, C.c_size_t, S, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t, C.c_void_p]
         f.restype = C.c_int
+    for p in "SDCZ":
+        S = _SCAL[p]
+        f = getattr(L, f"cu{p}trsm")
+        f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, S, C.c_uint64,
+                      C.c_size_t, C.c_uint64, C.c_size_t, C.c_void_p]
+        f.restype = C.c_int
+        f = getattr(L, f"cu{p}trmm2")
+        f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, S, C.c_uint64,
+                      C.c_size_t, C.c_uint64, C.c_size_t, C.c_uint64, C.c_size_t, C.c_void_p]
+        f.restype = C.c_int
     for name, p in (("cuSsyrk", "S"), ("cuDsyrk", "D"), ("cuCherk", "C"), ("cuZherk", "Z")):
         f = getattr(L, name)
         R = _REAL[p]
@@ -292,6 +303,20 @@ def call_gemm2(bh: BlasHandle, p: str, ta: str, tb: str, m: int, n: int, k: int,
                b: int, ldb: int, beta, c: int, ldc: int, d: int, ldd: int, stream: int = 0) -> int:
     return getattr(lib(), f"cu{p}gemm2")(bh.value, ord(ta), ord(tb), m, n, k, _scal(p, alpha), a, lda, b, ldb,
                                          _scal(p, beta), c, ldc, d, ldd, C.c_void_p(stream))
+
+
+def call_trsm(bh: BlasHandle, p: str, side: str, uplo: str, trans: str, diag: str, m: int, n: int, alpha,
+              a: int, lda: int, b: int, ldb: int, stream: int = 0) -> int:
+    """cu?trsm: B := alpha op(A)^-1 B (side L) or alpha B op(A)^-1 (side R), in place."""
+    return getattr(lib(), f"cu{p}trsm")(bh.value, ord(side), ord(uplo), ord(trans), ord(diag), m, n,
+                                        _scal(p, alpha), a, lda, b, ldb, C.c_void_p(stream))
+
+
+def call_trmm2(bh: BlasHandle, p: str, side: str, uplo: str, trans: str, diag: str, m: int, n: int, alpha,
+               a: int, lda: int, b: int, ldb: int, x: int, ldx: int, stream: int = 0) -> int:
+    """cu?trmm2: X := alpha op(A) B (side L) or alpha B op(A) (side R)."""
+    return getattr(lib(), f"cu{p}trmm2")(bh.value, ord(side), ord(uplo), ord(trans), ord(diag), m, n,
+                                         _scal(p, alpha), a, lda, b, ldb, x, ldx, C.c_void_p(stream))
 
 
 def call_rankk(bh: BlasHandle, p: str, uplo: str, trans: str, n: int, k: int, alpha: float, a: int, lda: int,

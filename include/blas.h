@@ -90,6 +90,29 @@ CUresult cuZgemm2(CUBLAShandle, CBlasTranspose, CBlasTranspose, size_t, size_t, 
                   cucholesky_cdouble, CUdeviceptr, size_t, CUdeviceptr, size_t,
                   cucholesky_cdouble, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
 
+/* Out-of-place triangular matrix multiply X := alpha op(A) B (side L) or alpha B op(A)
+ * (side R), A triangular (uplo, diag) (reference include/blas.h:214-232,
+ * blas/dtrmm.c:374). */
+CUresult cuStrmm2(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                  float, CUdeviceptr, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuDtrmm2(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                  double, CUdeviceptr, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuCtrmm2(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                  cucholesky_cfloat, CUdeviceptr, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuZtrmm2(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                  cucholesky_cdouble, CUdeviceptr, size_t, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+
+/* Triangular solve in place: B := alpha op(A)^-1 B (side L) or alpha B op(A)^-1
+ * (side R) (reference include/blas.h:235-253, blas/dtrsm.c:218). */
+CUresult cuStrsm(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                 float, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuDtrsm(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                 double, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuCtrsm(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                 cucholesky_cfloat, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+CUresult cuZtrsm(CUBLAShandle, CBlasSide, CBlasUplo, CBlasTranspose, CBlasDiag, size_t, size_t,
+                 cucholesky_cdouble, CUdeviceptr, size_t, CUdeviceptr, size_t, CUstream);
+
 #ifdef __cplusplus
 }
 #endif
