@@ -1,0 +1,332 @@
+// Host-memory routines of include/lapack.h and the device list of
+// include/cumultigpu.h (reference include/lapack.h:117-158, include/cumultigpu.h).
+//
+// The reference's cuMultiGPU?potrf (lapack/dpotrf.c:298-366) keeps A in host memory
+// for the whole factorization: every SYRK/GEMM/TRSM of the blocked algorithm is
+// tiled across the GPUs with its operand slabs staged from host memory per tile
+// (blas/dgemm.c:211-430), and each diagonal block is factored on the host.  On a
+// B200 one matrix of any size the reference handles fits in the GPU's 180 GB, so
+// the matrix crosses the bus once each way instead:
+//   1. the `uplo` triangle is copied to the GPU in 256-column blocks, each one 2-D
+//      copy of the block column's trapezoid (the other triangle crosses the bus only
+//      inside the diagonal blocks);
+//   2. the single-GPU driver runs on the copy (potrf_run, trtri_run, lauum_run);
+//   3. the triangle is copied back.  For ?potrf with page-locked (or device) memory
+//      the copy back of each block column is queued on a copy stream behind the work
+//      that finishes it, so all of it but the last block overlaps the factorization.
+//      Pageable memory is copied back after the driver (a copy to pageable memory
+//      returns only when it is done, which would stall the queueing of the schedule).
+// A call returns when its copies have landed.  The device buffer is cached in the
+// handle (grow-only, leading dimension rounded up to 32 elements).
+#pragma once
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t err;
+  explicit DeviceGuard(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    err = cudaSetDevice(d);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct __cumultigpu_st {
+  std::vector<int> devices;
+};
+
+struct __cumultigpulapackhandle_st {
+  int device;                   // the CUmultiGPU's first device
+  CULAPACKhandle h;             // single-GPU handle on that device
+  cudaStream_t s_copy;          // host <-> device copies
+  cudaEvent_t ev;
+  void* buf;                    // staged matrix (grow-only)
+  size_t buf_bytes;
+  unsigned long long h2d_bytes, d2h_bytes;   // bytes copied, since creation
+};
+
+namespace {
+
+constexpr size_t kStageCols = 256;   // columns per host <-> device copy
+
+CUresult stage_buffer(CUmultiGPULAPACKhandle hh, size_t bytes) {
+  if (bytes <= hh->buf_bytes) return CUDA_SUCCESS;
+  if (hh->buf != nullptr) {
+    CUCHOL_CHECK(cudaFree(hh->buf));
+    hh->buf = nullptr;
+    hh->buf_bytes = 0;
+  }
+  CUCHOL_CHECK(cudaMalloc(&hh->buf, bytes));
+  hh->buf_bytes = bytes;
+  return CUDA_SUCCESS;
+}
+
+// Page-locked host memory, device memory and managed memory take asynchronous
+// copies; pageable memory does not.
+bool async_copyable(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// The `uplo` triangle of an n x n column-major matrix, block column by block
+// column: lower, rows j .. n-1 of columns j .. j+w-1; upper, rows 0 .. j+w-1.
+template <typename T>
+CUresult copy_triangle(T* dst, size_t ldd, const T* src, size_t lds, size_t n, bool upper, cudaStream_t s,
+                       unsigned long long* bytes) {
+  for (size_t j = 0; j < n; j += kStageCols) {
+    const size_t w = std::min(kStageCols, n - j);
+    const size_t r0 = upper ? 0 : j, rows = upper ? j + w : n - j;
+    CUCHOL_CHECK(cudaMemcpy2DAsync(dst + r0 + j * ldd, ldd * sizeof(T), src + r0 + j * lds, lds * sizeof(T),
+                                   rows * sizeof(T), w, cudaMemcpyDefault, s));
+    *bytes += rows * w * sizeof(T);
+  }
+  return CUDA_SUCCESS;
+}
+
+// Copies the triangle in, and orders the handle's streams after the copies.
+template <typename T>
+CUresult stage_in(CUmultiGPULAPACKhandle hh, const T* A, size_t lda, size_t n, bool upper, T** D, size_t* ldd) {
+  *ldd = round_up(n, 32);
+  CUCHOL_CHECK_CU(stage_buffer(hh, sizeof(T) * *ldd * n));
+  *D = static_cast<T*>(hh->buf);
+  CUCHOL_CHECK_CU(copy_triangle<T>(*D, *ldd, A, lda, n, upper, hh->s_copy, &hh->h2d_bytes));
+  CUCHOL_CHECK(cudaEventRecord(hh->ev, hh->s_copy));
+  CUCHOL_CHECK(cudaStreamWaitEvent(hh->h->s_panel, hh->ev, 0));
+  CUCHOL_CHECK(cudaStreamWaitEvent(hh->h->s_update, hh->ev, 0));
+  return CUDA_SUCCESS;
+}
+
+// Ends a call: waits for the copy stream whatever happened before, and returns the
+// first error.
+inline CUresult finish(CUmultiGPULAPACKhandle hh, CUresult r) {
+  cudaError_t e = cudaStreamSynchronize(hh->s_copy);
+  if (r != CUDA_SUCCESS) return r;
+  CUCHOL_CHECK(e);
+  return CUDA_SUCCESS;
+}
+
+// Argument checks of the reference's host-memory drivers (lapack/dpotrf.c:302-308:
+// only lda, at position 4; position 5 for ?trtri).
+inline bool host_args(const char* name, size_t n, size_t lda, long pos, long* info) {
+  *info = 0;
+  if (lda < n) {
+    *info = -pos;
+    if (xerbla != nullptr) xerbla(name, pos);
+    return false;
+  }
+  return true;
+}
+
+template <typename T>
+CUresult host_potrf(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo, size_t n, T* A, size_t lda,
+                    long* info) {
+  if (!host_args(name, n, lda, 4, info)) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0) return CUDA_SUCCESS;
+  if (hh == nullptr || A == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  const bool upper = (uplo == CBlasUpper);
+  const bool overlap = async_copyable(A);
+  T* D;
+  size_t ldd;
+  CUresult r = stage_in<T>(hh, A, lda, n, upper, &D, &ldd);
+  if (r != CUDA_SUCCESS) return finish(hh, r);
+  // logical block column c .. c+jb-1, rows c .. n-1: physical columns of the lower
+  // triangle, physical rows of the upper one
+  FinalColumns back = [&](int c, int jb, cudaStream_t s) -> CUresult {
+    CUCHOL_CHECK(cudaEventRecord(hh->ev, s));
+    CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_copy, hh->ev, 0));
+    const size_t rows = n - (size_t)c, off = (size_t)c;
+    const size_t width = upper ? (size_t)jb : rows, height = upper ? rows : (size_t)jb;
+    CUCHOL_CHECK(cudaMemcpy2DAsync(A + off + off * lda, lda * sizeof(T), D + off + off * ldd, ldd * sizeof(T),
+                                   width * sizeof(T), height, cudaMemcpyDefault, hh->s_copy));
+    hh->d2h_bytes += rows * (size_t)jb * sizeof(T);
+    return CUDA_SUCCESS;
+  };
+  r = potrf_run<T>(hh->h, upper, (int)n, D, (long long)ldd, info, nullptr, overlap ? &back : nullptr);
+  if (r == CUDA_SUCCESS && !overlap) r = copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
+  CUCHOL_CHECK_CU(finish(hh, r));
+  return *info > 0 ? CUDA_ERROR_INVALID_VALUE : CUDA_SUCCESS;
+}
+
+template <typename T>
+CUresult host_trtri(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo, CBlasDiag diag, size_t n, T* A,
+                    size_t lda, long* info) {
+  if (!host_args(name, n, lda, 5, info)) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0) return CUDA_SUCCESS;
+  if (hh == nullptr || A == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  const bool upper = (uplo == CBlasUpper);
+  T* D;
+  size_t ldd;
+  CUresult r = stage_in<T>(hh, A, lda, n, upper, &D, &ldd);
+  if (r == CUDA_SUCCESS) r = trtri_run<T>(hh->h, upper, diag == CBlasUnit, (int)n, D, (long long)ldd, info);
+  // a singular matrix is left unmodified: nothing to copy back
+  if (r == CUDA_SUCCESS && *info == 0)
+    r = copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
+  CUCHOL_CHECK_CU(finish(hh, r));
+  return *info > 0 ? CUDA_ERROR_INVALID_VALUE : CUDA_SUCCESS;
+}
+
+template <typename T>
+CUresult host_lauum(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo, size_t n, T* A, size_t lda,
+                    long* info) {
+  if (!host_args(name, n, lda, 4, info)) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0) return CUDA_SUCCESS;
+  if (hh == nullptr || A == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  const bool upper = (uplo == CBlasUpper);
+  T* D;
+  size_t ldd;
+  CUresult r = stage_in<T>(hh, A, lda, n, upper, &D, &ldd);
+  if (r == CUDA_SUCCESS) r = lauum_run<T>(hh->h, upper, (int)n, D, (long long)ldd);
+  if (r == CUDA_SUCCESS) r = copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
+  return finish(hh, r);
+}
+
+template <typename T>
+CUresult host_potri(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo, size_t n, T* A, size_t lda,
+                    long* info) {
+  if (!host_args(name, n, lda, 4, info)) return CUDA_ERROR_INVALID_VALUE;
+  if (n == 0) return CUDA_SUCCESS;
+  if (hh == nullptr || A == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  const bool upper = (uplo == CBlasUpper);
+  T* D;
+  size_t ldd;
+  CUresult r = stage_in<T>(hh, A, lda, n, upper, &D, &ldd);
+  if (r == CUDA_SUCCESS) r = trtri_run<T>(hh->h, upper, false, (int)n, D, (long long)ldd, info);
+  if (r == CUDA_SUCCESS && *info == 0) r = lauum_run<T>(hh->h, upper, (int)n, D, (long long)ldd);
+  if (r == CUDA_SUCCESS && *info == 0)
+    r = copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
+  CUCHOL_CHECK_CU(finish(hh, r));
+  return *info > 0 ? CUDA_ERROR_INVALID_VALUE : CUDA_SUCCESS;
+}
+
+}  // namespace
+
+// ---- device list (reference include/cumultigpu.h:61-97) --------------------------
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPUCreate(CUmultiGPU* mgpu, CUdevice* devices, int n) {
+  if (mgpu == nullptr || devices == nullptr || n < 1) return CUDA_ERROR_INVALID_VALUE;
+  int count = 0;
+  CUCHOL_CHECK(cudaGetDeviceCount(&count));
+  for (int i = 0; i < n; ++i)
+    if (devices[i] < 0 || devices[i] >= count) return CUDA_ERROR_INVALID_DEVICE;
+  auto* m = new (std::nothrow) __cumultigpu_st;
+  if (m == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
+  m->devices.assign(devices, devices + n);
+  *mgpu = m;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPUDestroy(CUmultiGPU mgpu) {
+  if (mgpu == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  delete mgpu;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT int cuMultiGPUGetContextCount(CUmultiGPU mgpu) {
+  return mgpu == nullptr ? 0 : (int)mgpu->devices.size();
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPUSynchronize(CUmultiGPU mgpu) {
+  if (mgpu == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  for (int d : mgpu->devices) {
+    DeviceGuard g(d);
+    CUCHOL_CHECK(g.err);
+    CUCHOL_CHECK(cudaDeviceSynchronize());
+  }
+  return CUDA_SUCCESS;
+}
+
+// ---- host-memory LAPACK handle (reference include/lapack.h:119-122, lapack/handle.c:90-108)
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKCreate(CUmultiGPULAPACKhandle* handle, CUmultiGPU mgpu) {
+  if (handle == nullptr || mgpu == nullptr || mgpu->devices.empty()) return CUDA_ERROR_INVALID_VALUE;
+  auto* hh = new (std::nothrow) __cumultigpulapackhandle_st;
+  if (hh == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
+  memset(hh, 0, sizeof(*hh));
+  hh->device = mgpu->devices[0];
+  DeviceGuard g(hh->device);
+  CUresult r = (g.err == cudaSuccess) ? cuLAPACKCreate(&hh->h) : to_cu(g.err);
+  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithFlags(&hh->s_copy, cudaStreamNonBlocking));
+  if (r == CUDA_SUCCESS) r = to_cu(cudaEventCreateWithFlags(&hh->ev, cudaEventDisableTiming));
+  if (r != CUDA_SUCCESS) {
+    if (hh->ev) cudaEventDestroy(hh->ev);
+    if (hh->s_copy) cudaStreamDestroy(hh->s_copy);
+    if (hh->h) cuLAPACKDestroy(hh->h);
+    delete hh;
+    return r;
+  }
+  *handle = hh;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKDestroy(CUmultiGPULAPACKhandle hh) {
+  if (hh == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
+  if (hh->buf) cudaFree(hh->buf);
+  cudaEventDestroy(hh->ev);
+  cudaStreamDestroy(hh->s_copy);
+  CUresult r = cuLAPACKDestroy(hh->h);
+  delete hh;
+  return r;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKSynchronize(CUmultiGPULAPACKhandle hh) {
+  if (hh == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  DeviceGuard g(hh->device);
+  CUCHOL_CHECK(g.err);
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_panel));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_update));
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKGetStats(CUmultiGPULAPACKhandle hh, unsigned long long* launches,
+                                                           unsigned long long* h2d_bytes,
+                                                           unsigned long long* d2h_bytes) {
+  if (hh == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  if (launches) *launches = hh->h->launches;
+  if (h2d_bytes) *h2d_bytes = hh->h2d_bytes;
+  if (d2h_bytes) *d2h_bytes = hh->d2h_bytes;
+  return CUDA_SUCCESS;
+}
+
+#define CUCHOL_API_HOST(P, T, H)                                                                                  \
+  extern "C" CUCHOL_EXPORT CUresult cuMultiGPU##P##potrf(CUmultiGPULAPACKhandle h, CBlasUplo u, size_t n, H* A,  \
+                                                         size_t lda, long* info) {                               \
+    return host_potrf<T>("cuMultiGPU" #P "potrf", h, u, n, reinterpret_cast<T*>(A), lda, info);                  \
+  }                                                                                                               \
+  extern "C" CUCHOL_EXPORT CUresult cuMultiGPU##P##trtri(CUmultiGPULAPACKhandle h, CBlasUplo u, CBlasDiag d,     \
+                                                         size_t n, H* A, size_t lda, long* info) {               \
+    return host_trtri<T>("cuMultiGPU" #P "trtri", h, u, d, n, reinterpret_cast<T*>(A), lda, info);               \
+  }                                                                                                               \
+  extern "C" CUCHOL_EXPORT CUresult cuMultiGPU##P##lauum(CUmultiGPULAPACKhandle h, CBlasUplo u, size_t n, H* A,  \
+                                                         size_t lda, long* info) {                               \
+    return host_lauum<T>("cuMultiGPU" #P "lauum", h, u, n, reinterpret_cast<T*>(A), lda, info);                  \
+  }                                                                                                               \
+  extern "C" CUCHOL_EXPORT CUresult cuMultiGPU##P##potri(CUmultiGPULAPACKhandle h, CBlasUplo u, size_t n, H* A,  \
+                                                         size_t lda, long* info) {                               \
+    return host_potri<T>("cuMultiGPU" #P "potri", h, u, n, reinterpret_cast<T*>(A), lda, info);                  \
+  }
+CUCHOL_API_HOST(S, float, float)
+CUCHOL_API_HOST(D, double, double)
+CUCHOL_API_HOST(C, cuFloatComplex, cucholesky_cfloat)
+CUCHOL_API_HOST(Z, cuDoubleComplex, cucholesky_cdouble)

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <type_traits>
 #include <vector>
 
@@ -305,8 +306,15 @@ CUresult set_smem(const void* fn, size_t bytes) {
 // info word, and every later kernel exits at entry when it is set.
 constexpr int kDiagThreads2 = 256;
 
+// `on_final`, when given, is called once per diagonal block c .. c + jb - 1 in
+// order, as soon as the queued work that finishes that block column of the factor
+// (logical rows c .. n-1) has been issued, with the stream that work is on: a
+// caller can queue the copy of those columns behind it (host-memory routines).
+using FinalColumns = std::function<CUresult(int c, int jb, cudaStream_t s)>;
+
 template <typename T>
-CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out) {
+CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out,
+                   const FinalColumns* on_final = nullptr) {
   constexpr int nb = Tune<T>::nb;
   constexpr int NB = 2 * nb;
   using Smem = DiagSmem<T, nb>;
@@ -360,7 +368,10 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
           at(c, c), rs, cs, jb, (mr > 0 && !kReal) ? winv : nullptr, nb, c, d_info, h->d_logdet);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
-      if (mr == 0) break;
+      if (mr == 0) {
+        if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, sp));
+        break;
+      }
       // panel solve into P: rows c + jb .. n-1 are P rows s0 .. (P starts at j + nb)
       T* Ps = P + s0 + (long long)s0 * ldp;
       if constexpr (kReal) {
@@ -370,6 +381,7 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
         ++h->launches;
         CUCHOL_CHECK(cudaGetLastError());
         CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+        if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, sp));
       } else {
         GemmProblem<T> t = problem<T>();
         t.a = at(c + jb, c); t.a_rs = rs; t.a_ks = cs;
@@ -381,6 +393,7 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
         // update stream: the solved rows into A, off the panel stream's critical path
         CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
         CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
+        if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, su));
       }
       if (s0 == 0 && jB > nb) {
         // the second sub-panel's columns (rows j + nb ..) by the first sub-panel
@@ -940,3 +953,4 @@ CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 #include "batched.cuh"
 #include "mixed.cuh"
 #include "ozaki_driver.cuh"
+#include "hostmem.cuh"

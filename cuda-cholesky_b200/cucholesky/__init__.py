@@ -74,6 +74,9 @@ def exported_symbols() -> list[str]:
     for p in "SDCZ":
         names += [f"cu{p}{r}" for r in ("potrf", "trtri", "trti22", "lauum", "potri", "logdet", "gemm2", "trsm",
                                          "trmm2")]
+        names += [f"cuMultiGPU{p}{r}" for r in ("potrf", "trtri", "lauum", "potri")]
+    names += ["cuMultiGPUCreate", "cuMultiGPUDestroy", "cuMultiGPUGetContextCount", "cuMultiGPUSynchronize",
+              "cuMultiGPULAPACKCreate", "cuMultiGPULAPACKDestroy", "cuMultiGPULAPACKSynchronize"]
     return names
 
 
@@ -84,7 +87,7 @@ def extension_symbols() -> list[str]:
               "cuCholBatchedResults", "cuCholBatchedGetBlockSize", "cuCholBatchedDestroy", "cuDlogdetNoAlloc",
               "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
               "cuCholMixedGetFactor", "cuSsyrkLowp", "cuDpotrfOzaki",
-              "cuCholMixedDestroy", "cuDposvMixed"]
+              "cuCholMixedDestroy", "cuDposvMixed", "cuMultiGPULAPACKGetStats"]
     return names
 
 
@@ -508,3 +511,121 @@ def call_posv_mixed(h: Handle, uplo: str, n: int, nrhs: int, a: int, lda: int, b
     rc = L.cuDposvMixed(h.value, _uplo(uplo), n, nrhs, a, lda, b, ldb, x, ldx, precision, C.byref(it),
                         C.byref(berr), C.byref(info))
     return rc, it.value, berr.value, info.value
+
+
+# ---- host-memory routines (include/lapack.h cuMultiGPU*, include/cumultigpu.h) ----
+
+def _declare_host(L: C.CDLL) -> None:
+    if getattr(L, "_host_declared", False):
+        return
+    H = C.c_void_p
+    L.cuMultiGPUCreate.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_int]
+    L.cuMultiGPUDestroy.argtypes = [H]
+    L.cuMultiGPUGetContextCount.argtypes = [H]
+    L.cuMultiGPUSynchronize.argtypes = [H]
+    L.cuMultiGPULAPACKCreate.argtypes = [C.POINTER(C.c_void_p), H]
+    L.cuMultiGPULAPACKDestroy.argtypes = [H]
+    L.cuMultiGPULAPACKSynchronize.argtypes = [H]
+    L.cuMultiGPULAPACKGetStats.argtypes = [H] + [C.POINTER(C.c_ulonglong)] * 3
+    for f in (L.cuMultiGPUCreate, L.cuMultiGPUDestroy, L.cuMultiGPUGetContextCount, L.cuMultiGPUSynchronize,
+              L.cuMultiGPULAPACKCreate, L.cuMultiGPULAPACKDestroy, L.cuMultiGPULAPACKSynchronize,
+              L.cuMultiGPULAPACKGetStats):
+        f.restype = C.c_int
+    for p in "SDCZ":
+        for name in ("potrf", "lauum", "potri"):
+            f = getattr(L, f"cuMultiGPU{p}{name}")
+            f.argtypes = [H, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_long)]
+            f.restype = C.c_int
+        f = getattr(L, f"cuMultiGPU{p}trtri")
+        f.argtypes = [H, C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_long)]
+        f.restype = C.c_int
+    L._host_declared = True
+
+
+class MultiGPU:
+    """CUmultiGPU: the list of devices a host-memory handle may use."""
+
+    def __init__(self, devices=(0,)):
+        L = lib()
+        _declare_host(L)
+        self._m = C.c_void_p()
+        arr = (C.c_int * len(devices))(*devices)
+        rc = L.cuMultiGPUCreate(C.byref(self._m), arr, len(devices))
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuMultiGPUCreate", rc)
+
+    @property
+    def value(self) -> C.c_void_p:
+        return self._m
+
+    def count(self) -> int:
+        return lib().cuMultiGPUGetContextCount(self._m)
+
+    def synchronize(self) -> int:
+        return lib().cuMultiGPUSynchronize(self._m)
+
+    def close(self) -> None:
+        if self._m:
+            lib().cuMultiGPUDestroy(self._m)
+            self._m = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostHandle:
+    """CUmultiGPULAPACKhandle over a MultiGPU (host-memory ?potrf/?trtri/?lauum/?potri)."""
+
+    def __init__(self, mgpu: MultiGPU):
+        L = lib()
+        _declare_host(L)
+        self._h = C.c_void_p()
+        rc = L.cuMultiGPULAPACKCreate(C.byref(self._h), mgpu.value)
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuMultiGPULAPACKCreate", rc)
+
+    @property
+    def value(self) -> C.c_void_p:
+        return self._h
+
+    def synchronize(self) -> int:
+        return lib().cuMultiGPULAPACKSynchronize(self._h)
+
+    def stats(self) -> tuple[int, int, int]:
+        """(kernels launched, bytes host->device, bytes device->host) since creation."""
+        v = [C.c_ulonglong(0) for _ in range(3)]
+        rc = lib().cuMultiGPULAPACKGetStats(self._h, *[C.byref(x) for x in v])
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError("cuMultiGPULAPACKGetStats", rc)
+        return tuple(x.value for x in v)
+
+    def close(self) -> None:
+        if self._h:
+            lib().cuMultiGPULAPACKDestroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def call_host(hh, prefix: str, routine: str, uplo: str, n: int, ptr: int, lda: int,
+              diag: str = "N") -> tuple[int, int]:
+    """cuMultiGPU{prefix}{routine} on a column-major matrix at host address `ptr`
+    (a numpy array's ``ctypes.data`` or a pinned torch tensor's ``data_ptr()``);
+    returns (CUresult, info).  `hh` may be None to exercise the argument checks."""
+    L = lib()
+    _declare_host(L)
+    info = C.c_long(0)
+    f = getattr(L, f"cuMultiGPU{prefix}{routine}")
+    h = hh.value if hh is not None else None
+    if routine == "trtri":
+        rc = f(h, _uplo(uplo), ord(diag.upper()), n, ptr, lda, C.byref(info))
+    else:
+        rc = f(h, _uplo(uplo), n, ptr, lda, C.byref(info))
+    return rc, info.value

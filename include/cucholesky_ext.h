@@ -137,6 +137,12 @@ CUresult cuSsyrkLowp(CULAPACKhandle, int, size_t, size_t, float, CUdeviceptr, si
  * products are exact INT32 sums, and only the final FP64 combination rounds (7 or 8
  * slices: FP64-level backward error).  No counterpart in the reference library. */
 CUresult cuDpotrfOzaki(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, int, long *);
+
+/* Counters of a host-memory handle since its creation (for measurement): kernels
+ * launched, and bytes copied host -> device and device -> host.  Any pointer may be
+ * NULL. */
+CUresult cuMultiGPULAPACKGetStats(CUmultiGPULAPACKhandle, unsigned long long *, unsigned long long *,
+                                  unsigned long long *);
 #ifdef __cplusplus
 }
 #endif

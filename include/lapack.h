@@ -5,9 +5,9 @@
  *
  * Every prototype below is identical to the one in the reference's
  * include/lapack.h (line numbers cited per entry), so code written against the
- * reference's GPU routines links against this library unchanged.  The reference's
- * CPU routines (spotrf ... zpotri, ?logdet) and its cuMultiGPU* routines are not
- * exported by this library.
+ * reference's GPU routines, and against its host-memory cuMultiGPU* routines,
+ * links against this library unchanged.  The reference's CPU routines
+ * (spotrf ... zpotri, ?logdet) are not exported by this library.
  *
  * Conventions kept from the reference:
  *   - column-major storage, only the `uplo` triangle is read or written;
@@ -29,6 +29,13 @@
 #define CUCHOLESKY_LAPACK_H
 
 #include "blas.h"
+#include "cumultigpu.h"
+
+#ifdef __cplusplus
+#define CUCHOLESKY_RESTRICT __restrict__
+#else
+#define CUCHOLESKY_RESTRICT restrict
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -91,6 +98,46 @@ CUresult cuSlogdet(CULAPACKhandle, CUdeviceptr, size_t, size_t,  float *, CUstre
 CUresult cuDlogdet(CULAPACKhandle, CUdeviceptr, size_t, size_t, double *, CUstream);
 CUresult cuClogdet(CULAPACKhandle, CUdeviceptr, size_t, size_t,  float *, CUstream);
 CUresult cuZlogdet(CULAPACKhandle, CUdeviceptr, size_t, size_t, double *, CUstream);
+
+/* Host-memory routines (reference include/lapack.h:117-158).  A is a host array
+ * (pageable or page-locked; a device or managed pointer also works); the call
+ * copies the `uplo` triangle to the first device of the handle's CUmultiGPU, runs
+ * the single-GPU routine there and copies the triangle back before it returns.
+ * With page-locked A, cu?potrf copies each block column of the factor back while
+ * the rest of the factorization runs.  Same argument checks as the reference
+ * (lda < n: info -4, -5 for ?trtri); numerical failure (info > 0) returns
+ * CUDA_ERROR_INVALID_VALUE as the reference's host-memory routines do
+ * (lapack/dpotrf.c:331, lapack/dtrtri.c:498, lapack/dpotri.c:64), and a singular
+ * ?trtri leaves A unmodified.  The handle caches one device buffer of the largest
+ * matrix seen; calls on one handle must not overlap. */
+typedef struct __cumultigpulapackhandle_st * CUmultiGPULAPACKhandle;
+CUresult cuMultiGPULAPACKCreate(CUmultiGPULAPACKhandle *, CUmultiGPU);   /* lapack.h:120 */
+CUresult cuMultiGPULAPACKDestroy(CUmultiGPULAPACKhandle);                /* lapack.h:121 */
+CUresult cuMultiGPULAPACKSynchronize(CUmultiGPULAPACKhandle);            /* lapack.h:122 */
+
+/* Cholesky factor in host memory (reference include/lapack.h:124-131, lapack/dpotrf.c:298). */
+CUresult cuMultiGPUSpotrf(CUmultiGPULAPACKhandle, CBlasUplo, size_t, float * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUDpotrf(CUmultiGPULAPACKhandle, CBlasUplo, size_t, double * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUCpotrf(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cfloat * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUZpotrf(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cdouble * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+
+/* Triangular inverse in host memory (reference include/lapack.h:133-140, lapack/dtrtri.c:470). */
+CUresult cuMultiGPUStrtri(CUmultiGPULAPACKhandle, CBlasUplo, CBlasDiag, size_t, float * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUDtrtri(CUmultiGPULAPACKhandle, CBlasUplo, CBlasDiag, size_t, double * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUCtrtri(CUmultiGPULAPACKhandle, CBlasUplo, CBlasDiag, size_t, cucholesky_cfloat * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUZtrtri(CUmultiGPULAPACKhandle, CBlasUplo, CBlasDiag, size_t, cucholesky_cdouble * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+
+/* Triangular square in host memory (reference include/lapack.h:142-149, lapack/dlauum.c:294). */
+CUresult cuMultiGPUSlauum(CUmultiGPULAPACKhandle, CBlasUplo, size_t, float * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUDlauum(CUmultiGPULAPACKhandle, CBlasUplo, size_t, double * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUClauum(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cfloat * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUZlauum(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cdouble * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+
+/* Inverse from the Cholesky factor in host memory (reference include/lapack.h:151-158, lapack/dpotri.c:48). */
+CUresult cuMultiGPUSpotri(CUmultiGPULAPACKhandle, CBlasUplo, size_t, float * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUDpotri(CUmultiGPULAPACKhandle, CBlasUplo, size_t, double * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUCpotri(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cfloat * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
+CUresult cuMultiGPUZpotri(CUmultiGPULAPACKhandle, CBlasUplo, size_t, cucholesky_cdouble * CUCHOLESKY_RESTRICT, size_t, long * CUCHOLESKY_RESTRICT);
 
 #ifdef __cplusplus
 }

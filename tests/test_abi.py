@@ -136,3 +136,66 @@ def test_extension_argument_errors():
         assert info.value == -5
     finally:
         xer.value = old
+
+
+@pytest.mark.parametrize("p", list("SDCZ"))
+def test_host_memory_argument_errors(p):
+    """cuMultiGPU?potrf/?lauum/?potri check lda first (info -4, XERBLA position 4),
+    ?trtri at position 5 (lapack/dpotrf.c:302-308, lapack/dtrtri.c:475-481); n = 0
+    succeeds; a NULL handle or matrix is CUDA_ERROR_INVALID_VALUE.  No GPU touched."""
+    lib = cucholesky.lib()
+    calls = []
+    XERBLA = C.CFUNCTYPE(None, C.c_char_p, C.c_long)
+
+    def hook(name, info):
+        calls.append((name.decode(), info))
+
+    cb = XERBLA(hook)
+    xer = C.c_void_p.in_dll(lib, "xerbla")
+    old = xer.value
+    xer.value = C.cast(cb, C.c_void_p).value
+    try:
+        for name, pos in (("potrf", 4), ("lauum", 4), ("potri", 4), ("trtri", 5)):
+            rc, info = cucholesky.call_host(None, p, name, "L", 10, 0, 5)
+            assert rc == cucholesky.CUDA_ERROR_INVALID_VALUE and info == -pos
+            assert calls[-1] == (f"cuMultiGPU{p}{name}", pos)
+            assert cucholesky.call_host(None, p, name, "U", 0, 0, 0) == (0, 0)
+            n_calls = len(calls)
+            rc, info = cucholesky.call_host(None, p, name, "L", 10, 0, 10)
+            assert rc == cucholesky.CUDA_ERROR_INVALID_VALUE and info == 0
+            assert len(calls) == n_calls
+    finally:
+        xer.value = old
+
+
+def test_device_list_argument_errors():
+    lib = cucholesky.lib()
+    cucholesky._declare_host(lib)
+    m = C.c_void_p()
+    assert lib.cuMultiGPUCreate(None, None, 1) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    devs = (C.c_int * 1)(0)
+    assert lib.cuMultiGPUCreate(C.byref(m), devs, 0) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    assert lib.cuMultiGPUGetContextCount(None) == 0
+    assert lib.cuMultiGPUDestroy(None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    assert lib.cuMultiGPUSynchronize(None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    hh = C.c_void_p()
+    assert lib.cuMultiGPULAPACKCreate(C.byref(hh), None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    assert lib.cuMultiGPULAPACKDestroy(None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    assert lib.cuMultiGPULAPACKSynchronize(None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_headers_compile(tmp_path, lang):
+    """include/*.h are drop-in C99 and C++ headers (the reference's are C)."""
+    import shutil
+    cc_ = shutil.which("gcc" if lang == "c" else "g++")
+    cuda_inc = "/usr/local/cuda/include"
+    if cc_ is None or not os.path.exists(os.path.join(cuda_inc, "cuda.h")):
+        pytest.skip("no host compiler or CUDA headers")
+    src = tmp_path / ("h.c" if lang == "c" else "h.cpp")
+    src.write_text('#include "lapack.h"\n#include "cucholesky_ext.h"\n#include "cumultigpu.h"\n'
+                   "int main(void) { CUmultiGPULAPACKhandle h = 0; (void)h; return (int)CBlasLower - 'L'; }\n")
+    std = ["-std=c99"] if lang == "c" else ["-std=c++17"]
+    r = subprocess.run([cc_, *std, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                        "-c", str(src), "-o", str(tmp_path / "h.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
