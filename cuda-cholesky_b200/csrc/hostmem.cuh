@@ -11,11 +11,19 @@
 //      copy of the block column's trapezoid (the other triangle crosses the bus only
 //      inside the diagonal blocks);
 //   2. the single-GPU driver runs on the copy (potrf_run, trtri_run, lauum_run);
-//   3. the triangle is copied back.  For ?potrf with page-locked (or device) memory
-//      the copy back of each block column is queued on a copy stream behind the work
-//      that finishes it, so all of it but the last block overlaps the factorization.
-//      Pageable memory is copied back after the driver (a copy to pageable memory
-//      returns only when it is done, which would stall the queueing of the schedule).
+//   3. the triangle is copied back.
+// ?potrf with page-locked (or device) memory overlaps both copies with the
+// factorization.  Copy back: each block column of the factor is queued on an
+// outbound copy stream behind the work that finishes it.  Copy in: the matrix is
+// cut into tall panels (1024 columns wide up to the middle column, then the rest in
+// one), copied in that order, and factored left-looking panel by panel as they
+// land: a panel first receives the updates of every column left of it in one GEMM
+// (K = its first column), then potrf_run factors it as a tall panel (right-looking
+// inside, trailing updates restricted to its own columns).  The first panels hold
+// most of the bytes and little of the work, so the work waiting for the last copy
+// is the right-looking factorization of the second half.  Pageable memory is
+// copied in before and back after the driver (a copy to pageable memory returns
+// only when it is done, which would stall the queueing of the schedule).
 // A call returns when its copies have landed.  The device buffer is cached in the
 // handle (grow-only, leading dimension rounded up to 32 elements).
 #pragma once
@@ -44,13 +52,18 @@ struct __cumultigpu_st {
 };
 
 struct __cumultigpulapackhandle_st {
-  int device;                   // the CUmultiGPU's first device
-  CULAPACKhandle h;             // single-GPU handle on that device
-  cudaStream_t s_copy;          // host <-> device copies
-  cudaEvent_t ev;
-  void* buf;                    // staged matrix (grow-only)
-  size_t buf_bytes;
-  unsigned long long h2d_bytes, d2h_bytes;   // bytes copied, since creation
+  int device = 0;                   // the CUmultiGPU's first device
+  CULAPACKhandle h = nullptr;       // single-GPU handle on that device
+  cudaStream_t s_copy = nullptr;    // host -> device copies (and all copies of the
+                                    // routines that do not overlap them)
+  cudaStream_t s_out = nullptr;     // device -> host copies overlapped with ?potrf
+  cudaEvent_t ev = nullptr;
+  cudaStream_t s_gemm = nullptr;    // ?potrf: updates of the next tall panel (low priority)
+  std::vector<cudaEvent_t> ev_in;   // one per tall panel copied in
+  std::vector<cudaEvent_t> ev_a;    // one per tall panel: its early updates are done
+  void* buf = nullptr;              // staged matrix (grow-only)
+  size_t buf_bytes = 0;
+  unsigned long long h2d_bytes = 0, d2h_bytes = 0;   // bytes copied, since creation
 };
 
 namespace {
@@ -95,6 +108,22 @@ CUresult copy_triangle(T* dst, size_t ldd, const T* src, size_t lds, size_t n, b
   return CUDA_SUCCESS;
 }
 
+// Logical block columns c0 .. c1-1 of the `uplo` triangle, logical rows from each
+// piece's first column down: lower, physical columns (rows j .. n-1 of columns
+// j .. j+w-1); upper, physical rows (columns j .. n-1 of rows j .. j+w-1).
+template <typename T>
+CUresult copy_panel(T* dst, size_t ldd, const T* src, size_t lds, size_t n, bool upper, size_t c0, size_t c1,
+                    cudaStream_t s, unsigned long long* bytes) {
+  for (size_t j = c0; j < c1; j += kStageCols) {
+    const size_t w = std::min(kStageCols, c1 - j), len = n - j;
+    const size_t width = upper ? w : len, height = upper ? len : w;
+    CUCHOL_CHECK(cudaMemcpy2DAsync(dst + j + j * ldd, ldd * sizeof(T), src + j + j * lds, lds * sizeof(T),
+                                   width * sizeof(T), height, cudaMemcpyDefault, s));
+    *bytes += len * w * sizeof(T);
+  }
+  return CUDA_SUCCESS;
+}
+
 // Copies the triangle in, and orders the handle's streams after the copies.
 template <typename T>
 CUresult stage_in(CUmultiGPULAPACKhandle hh, const T* A, size_t lda, size_t n, bool upper, T** D, size_t* ldd) {
@@ -108,13 +137,28 @@ CUresult stage_in(CUmultiGPULAPACKhandle hh, const T* A, size_t lda, size_t n, b
   return CUDA_SUCCESS;
 }
 
-// Ends a call: waits for the copy stream whatever happened before, and returns the
+// Ends a call: waits for the copy streams whatever happened before, and returns the
 // first error.
 inline CUresult finish(CUmultiGPULAPACKhandle hh, CUresult r) {
   cudaError_t e = cudaStreamSynchronize(hh->s_copy);
+  cudaError_t e2 = cudaStreamSynchronize(hh->s_out);
+  cudaError_t e3 = cudaStreamSynchronize(hh->s_gemm);
   if (r != CUDA_SUCCESS) return r;
   CUCHOL_CHECK(e);
+  CUCHOL_CHECK(e2);
+  CUCHOL_CHECK(e3);
   return CUDA_SUCCESS;
+}
+
+constexpr size_t kPanelCols = 1024;    // tall-panel width of the streamed ?potrf
+
+// Column boundaries of the tall panels: 1024 wide while the panel ends at or
+// before the middle column, then one panel to the end.
+inline std::vector<size_t> panel_plan(size_t n) {
+  std::vector<size_t> b{0};
+  while (b.back() + kPanelCols <= n / 2) b.push_back(b.back() + kPanelCols);
+  if (b.back() < n) b.push_back(n);
+  return b;
 }
 
 // Argument checks of the reference's host-memory drivers (lapack/dpotrf.c:302-308:
@@ -130,6 +174,91 @@ inline bool host_args(const char* name, size_t n, size_t lda, long pos, long* in
 }
 
 template <typename T>
+CUresult host_potrf_run(CUmultiGPULAPACKhandle hh, bool upper, size_t n, T* A, size_t lda, long* info) {
+  CULAPACKhandle h = hh->h;
+  const size_t ldd = round_up(n, 32);
+  CUCHOL_CHECK_CU(stage_buffer(hh, sizeof(T) * ldd * n));
+  T* D = static_cast<T*>(hh->buf);
+  const long long rs = upper ? (long long)ldd : 1, cs = upper ? 1 : (long long)ldd;
+  auto at = [&](size_t i, size_t j) { return D + (long long)i * rs + (long long)j * cs; };
+  if (!async_copyable(A)) {
+    // pageable: copy in, factor, copy back
+    CUCHOL_CHECK_CU(copy_triangle<T>(D, ldd, A, lda, n, upper, hh->s_copy, &hh->h2d_bytes));
+    CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
+    CUCHOL_CHECK_CU(potrf_run<T>(h, upper, (int)n, D, (long long)ldd, info, nullptr));
+    return copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
+  }
+  const std::vector<size_t> plan = panel_plan(n);
+  const size_t panels = plan.size() - 1;
+  while (hh->ev_in.size() < panels) {
+    cudaEvent_t e;
+    CUCHOL_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    hh->ev_in.push_back(e);
+  }
+  // every copy in is queued at once, in panel order
+  for (size_t r = 0; r < panels; ++r) {
+    CUCHOL_CHECK_CU(copy_panel<T>(D, ldd, A, lda, n, upper, plan[r], plan[r + 1], hh->s_copy, &hh->h2d_bytes));
+    CUCHOL_CHECK(cudaEventRecord(hh->ev_in[r], hh->s_copy));
+  }
+  while (hh->ev_a.size() < panels) {
+    cudaEvent_t e;
+    CUCHOL_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    hh->ev_a.push_back(e);
+  }
+  const T minus_one = from_real<T>(RealOf<T>(-1)), one = from_real<T>(RealOf<T>(1));
+  // A(c0:, c0:c0+w) -= L(c0:, k0:k1) L(c0:c0+w, k0:k1)^H, lower-only on the panel's
+  // diagonal block
+  auto catch_up = [&](size_t c0, size_t w, size_t k0, size_t k1, cudaStream_t s) -> CUresult {
+    if (k1 <= k0) return CUDA_SUCCESS;
+    GemmProblem<T> u = problem<T>();
+    u.a = at(c0, k0); u.a_rs = rs; u.a_ks = cs;
+    u.b = at(c0, k0); u.b_rs = rs; u.b_ks = cs; u.conj_b = 1;
+    u.c = at(c0, c0); u.c_rs = rs; u.c_cs = cs;
+    u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
+    u.alpha = minus_one; u.beta = one;
+    u.lower_only = 1; u.real_diag = 1;
+    u.m = (int)(n - c0); u.n = (int)w; u.k = (int)(k1 - k0);
+    return gemm<T>(h, u, s, nullptr);
+  };
+  // Panel r receives the updates of columns 0 .. plan[r-1]-1 on the low-priority
+  // stream while panel r-1 is factored (those columns are final by then), and the
+  // updates of panel r-1's columns on the panel stream after it.
+  for (size_t r = 0; r < panels; ++r) {
+    const size_t c0 = plan[r], w = plan[r + 1] - c0;
+    CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_in[r], 0));
+    CUCHOL_CHECK(cudaStreamWaitEvent(h->s_update, hh->ev_in[r], 0));
+    if (r >= 1) {
+      if (r >= 2) CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_a[r], 0));
+      CUCHOL_CHECK_CU(catch_up(c0, w, plan[r - 1], c0, h->s_panel));
+    }
+    if (r + 1 < panels && r >= 1) {
+      CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_gemm, hh->ev_in[r + 1], 0));
+      CUCHOL_CHECK_CU(catch_up(plan[r + 1], plan[r + 2] - plan[r + 1], 0, c0, hh->s_gemm));
+      CUCHOL_CHECK(cudaEventRecord(hh->ev_a[r + 1], hh->s_gemm));
+    }
+    FinalColumns back = [&](int c, int jb, cudaStream_t s) -> CUresult {
+      CUCHOL_CHECK(cudaEventRecord(hh->ev, s));
+      CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_out, hh->ev, 0));
+      const size_t g = c0 + (size_t)c, rows = n - g;
+      const size_t width = upper ? (size_t)jb : rows, height = upper ? rows : (size_t)jb;
+      CUCHOL_CHECK(cudaMemcpy2DAsync(A + g + g * lda, lda * sizeof(T), D + g + g * ldd, ldd * sizeof(T),
+                                     width * sizeof(T), height, cudaMemcpyDefault, hh->s_out));
+      hh->d2h_bytes += rows * (size_t)jb * sizeof(T);
+      return CUDA_SUCCESS;
+    };
+    long pinfo = 0;
+    CUCHOL_CHECK_CU(potrf_run<T>(h, upper, (int)(n - c0), at(c0, c0), (long long)ldd, &pinfo, nullptr, &back,
+                                 (int)w));
+    if (pinfo != 0) {
+      *info = (long)c0 + pinfo;
+      return CUDA_SUCCESS;
+    }
+  }
+  *info = 0;
+  return CUDA_SUCCESS;
+}
+
+template <typename T>
 CUresult host_potrf(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo, size_t n, T* A, size_t lda,
                     long* info) {
   if (!host_args(name, n, lda, 4, info)) return CUDA_ERROR_INVALID_VALUE;
@@ -137,27 +266,7 @@ CUresult host_potrf(const char* name, CUmultiGPULAPACKhandle hh, CBlasUplo uplo,
   if (hh == nullptr || A == nullptr || bad_uplo(uplo) || n > (size_t)INT_MAX) return CUDA_ERROR_INVALID_VALUE;
   DeviceGuard g(hh->device);
   CUCHOL_CHECK(g.err);
-  const bool upper = (uplo == CBlasUpper);
-  const bool overlap = async_copyable(A);
-  T* D;
-  size_t ldd;
-  CUresult r = stage_in<T>(hh, A, lda, n, upper, &D, &ldd);
-  if (r != CUDA_SUCCESS) return finish(hh, r);
-  // logical block column c .. c+jb-1, rows c .. n-1: physical columns of the lower
-  // triangle, physical rows of the upper one
-  FinalColumns back = [&](int c, int jb, cudaStream_t s) -> CUresult {
-    CUCHOL_CHECK(cudaEventRecord(hh->ev, s));
-    CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_copy, hh->ev, 0));
-    const size_t rows = n - (size_t)c, off = (size_t)c;
-    const size_t width = upper ? (size_t)jb : rows, height = upper ? rows : (size_t)jb;
-    CUCHOL_CHECK(cudaMemcpy2DAsync(A + off + off * lda, lda * sizeof(T), D + off + off * ldd, ldd * sizeof(T),
-                                   width * sizeof(T), height, cudaMemcpyDefault, hh->s_copy));
-    hh->d2h_bytes += rows * (size_t)jb * sizeof(T);
-    return CUDA_SUCCESS;
-  };
-  r = potrf_run<T>(hh->h, upper, (int)n, D, (long long)ldd, info, nullptr, overlap ? &back : nullptr);
-  if (r == CUDA_SUCCESS && !overlap) r = copy_triangle<T>(A, lda, D, ldd, n, upper, hh->s_copy, &hh->d2h_bytes);
-  CUCHOL_CHECK_CU(finish(hh, r));
+  CUCHOL_CHECK_CU(finish(hh, host_potrf_run<T>(hh, uplo == CBlasUpper, n, A, lda, info)));
   return *info > 0 ? CUDA_ERROR_INVALID_VALUE : CUDA_SUCCESS;
 }
 
@@ -257,16 +366,21 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPUSynchronize(CUmultiGPU mgpu) {
 // ---- host-memory LAPACK handle (reference include/lapack.h:119-122, lapack/handle.c:90-108)
 extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKCreate(CUmultiGPULAPACKhandle* handle, CUmultiGPU mgpu) {
   if (handle == nullptr || mgpu == nullptr || mgpu->devices.empty()) return CUDA_ERROR_INVALID_VALUE;
-  auto* hh = new (std::nothrow) __cumultigpulapackhandle_st;
+  auto* hh = new (std::nothrow) __cumultigpulapackhandle_st();
   if (hh == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
-  memset(hh, 0, sizeof(*hh));
   hh->device = mgpu->devices[0];
   DeviceGuard g(hh->device);
   CUresult r = (g.err == cudaSuccess) ? cuLAPACKCreate(&hh->h) : to_cu(g.err);
   if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithFlags(&hh->s_copy, cudaStreamNonBlocking));
+  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithFlags(&hh->s_out, cudaStreamNonBlocking));
+  int lo = 0, hi = 0;
+  if (r == CUDA_SUCCESS) r = to_cu(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithPriority(&hh->s_gemm, cudaStreamNonBlocking, lo));
   if (r == CUDA_SUCCESS) r = to_cu(cudaEventCreateWithFlags(&hh->ev, cudaEventDisableTiming));
   if (r != CUDA_SUCCESS) {
     if (hh->ev) cudaEventDestroy(hh->ev);
+    if (hh->s_out) cudaStreamDestroy(hh->s_out);
+    if (hh->s_gemm) cudaStreamDestroy(hh->s_gemm);
     if (hh->s_copy) cudaStreamDestroy(hh->s_copy);
     if (hh->h) cuLAPACKDestroy(hh->h);
     delete hh;
@@ -281,8 +395,14 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKDestroy(CUmultiGPULAPACKhandle
   DeviceGuard g(hh->device);
   CUCHOL_CHECK(g.err);
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_out));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_gemm));
   if (hh->buf) cudaFree(hh->buf);
   cudaEventDestroy(hh->ev);
+  for (cudaEvent_t e : hh->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : hh->ev_a) cudaEventDestroy(e);
+  cudaStreamDestroy(hh->s_gemm);
+  cudaStreamDestroy(hh->s_out);
   cudaStreamDestroy(hh->s_copy);
   CUresult r = cuLAPACKDestroy(hh->h);
   delete hh;
@@ -294,6 +414,8 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKSynchronize(CUmultiGPULAPACKha
   DeviceGuard g(hh->device);
   CUCHOL_CHECK(g.err);
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_out));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_gemm));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_panel));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_update));
   return CUDA_SUCCESS;

@@ -310,11 +310,15 @@ constexpr int kDiagThreads2 = 256;
 // order, as soon as the queued work that finishes that block column of the factor
 // (logical rows c .. n-1) has been issued, with the stream that work is on: a
 // caller can queue the copy of those columns behind it (host-memory routines).
+// `ncols` < n factors only the leading ncols columns of the n x n trailing matrix
+// (a tall panel: its diagonal blocks, the solves below them, and the updates of its
+// own columns); the columns right of it are neither read nor written.
 using FinalColumns = std::function<CUresult(int c, int jb, cudaStream_t s)>;
 
 template <typename T>
 CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, long* info, double* logdet_out,
-                   const FinalColumns* on_final = nullptr) {
+                   const FinalColumns* on_final = nullptr, int ncols = -1) {
+  if (ncols < 0 || ncols > n) ncols = n;
   constexpr int nb = Tune<T>::nb;
   constexpr int NB = 2 * nb;
   using Smem = DiagSmem<T, nb>;
@@ -357,9 +361,10 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
     return gemm<T>(h, u, s, d_info);
   };
 
-  for (int j = 0, step = 0; j < n; j += NB, ++step) {
-    const int jB = std::min(NB, n - j);
+  for (int j = 0, step = 0; j < ncols; j += NB, ++step) {
+    const int jB = std::min(NB, ncols - j);
     const int m = n - j - jB;                    // rows below the outer block
+    const int mc = ncols - j - jB;               // columns right of it (in the panel)
     T* P = pbuf[step & 1];
     for (int s0 = 0; s0 < jB; s0 += nb) {
       const int c = j + s0, jb = std::min(nb, j + jB - c);
@@ -400,16 +405,17 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
         CUCHOL_CHECK_CU(update(j + nb, j + nb, n - j - nb, jB - nb, P, P, nb, sp));
       }
     }
-    if (m == 0) break;
+    if (m == 0 || mc == 0) break;
     // lookahead: next outer block (P rows from j + NB, k = jB), after the previous
     // trailing update
-    const int jB2 = std::min(NB, m);
+    const int jB2 = std::min(NB, mc);
     const T* Pt = P + nb;
     CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
     CUCHOL_CHECK_CU(update(j + NB, j + NB, m, jB2, Pt, Pt, jB, sp));
     // rest of the trailing matrix, once P holds both sub-panels
     CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
-    if (m > jB2) CUCHOL_CHECK_CU(update(j + NB + jB2, j + NB + jB2, m - jB2, m - jB2, Pt + jB2, Pt + jB2, jB, su));
+    if (mc > jB2)
+      CUCHOL_CHECK_CU(update(j + NB + jB2, j + NB + jB2, m - jB2, mc - jB2, Pt + jB2, Pt + jB2, jB, su));
     // always recorded: it also covers the copies that still read P
     CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   }

@@ -9,13 +9,16 @@
 //                       triangular matrix (the leaves of the recursive ?TRTRI).
 //
 // Both work on the block in shared memory in 32-column sub-blocks:
-//   * one warp factors a 32 x 32 sub-block with its rows in registers (pivot and
-//     column broadcast by warp shuffles), then inverts it (one column per lane);
-//   * the other work is register-tiled SIMT products over shared memory: the
-//     left-looking update of the next sub-block column, the solve of the rows below
-//     a sub-block (times the inverted sub-block), and the block-column assembly of
-//     inv(L) from the last column block back (the order of the reference's lower
-//     dtrtri, lapack/dtrtri.c:141-162).
+//   * the factor takes the block one 32-column sub-panel (the sub-block column from
+//     its diagonal down) at a time: a left-looking register-tiled update by the
+//     columns before it, then a right-looking factor of the sub-panel by all 256
+//     threads, each holding 16 elements of one row in registers, one pivot per
+//     step and one barrier per step (the next pivot column is published to shared
+//     memory by the update that finishes it);
+//   * the inverse (when asked for) inverts each 32 x 32 diagonal sub-block with one
+//     warp (one column per lane) and assembles inv(L) block column by block column
+//     from the last one back (the order of the reference's lower dtrtri,
+//     lapack/dtrtri.c:141-162) with register-tiled SIMT products.
 // The diagonal block is factored on the GPU next to the trailing update; the
 // reference copied it to the host for a CPU dpotrf every step
 // (lapack/dpotrf.c:263-276).
@@ -65,79 +68,106 @@ struct DiagSmem {
   static constexpr int TLD = NB / 2 + 1;               // TMP: (NB/2) x (NB/2), row-major
   static constexpr size_t TMP = sizeof(T) * (NB / 2) * TLD;
   static constexpr size_t R = sizeof(T) * NB;         // reciprocal pivots
-  static constexpr size_t bytes = S + X + TMP + R + 16;
+  static constexpr size_t C = sizeof(T) * 2 * 128;    // pivot columns (double-buffered)
+  static constexpr size_t bytes = S + X + TMP + R + C + 16;
 };
 
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
 
-// Warp: Cholesky of the pb x pb sub-block at (c0, c0) of S, lower part, in place.
-// (The three warp routines are not inlined: compiled as separate functions each
-// keeps its 32-element array in registers.)
-// Lane i holds row i in registers; both loops are unrolled so every index is a
-// compile-time register name (no window shifting): per pivot, one shuffle of the
-// pivot, one rsqrt, then 31-k independent shuffle + FMA pairs.  rdiag[c0+k] =
-// 1 / L(k,k).  Returns the first failing local column (pivot <= 0 or NaN) or -1;
-// on failure the columns before it are factored and the rest is left as updated.
+// 16 consecutive shared-memory elements from a 16-byte aligned address, in
+// 16-byte loads.
 template <typename T>
-__device__ __noinline__ int warp_chol32(T* S, int LD, int c0, int pb, T* rdiag) {
-  using R = RealOf<T>;
-  const int i = threadIdx.x & 31;
-  T a[32];
+__device__ __forceinline__ void load16(const T* p, T (&v)[16]) {
+  static_assert(16 % sizeof(T) == 0, "element of 4, 8 or 16 bytes");
+  constexpr int per = 16 / sizeof(T);
+  const int4* q = reinterpret_cast<const int4*>(p);
 #pragma unroll
-  for (int j = 0; j < 32; ++j) a[j] = (i < pb && j <= i) ? S[(c0 + j) * LD + c0 + i] : zero<T>();
-  int fail = -1;
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    if (k < pb && fail < 0) {                     // warp-uniform
-      const R d = re(shfl(a[k], k));
-      if (!(d > R(0))) {
-        fail = k;
-      } else {
-        const R r = rsqrt_(d);
-        const T l = (i == k) ? from_real<T>(d * r) : scale(a[k], r);
-        if (i == k) rdiag[c0 + k] = from_real<T>(r);
-#pragma unroll
-        for (int j = k + 1; j < 32; ++j) {
-          const T lj = shfl(l, j);
-          if (i >= j) mac(a[j], neg(l), cj(lj));
-        }
-        if (i >= k) a[k] = l;
-      }
-    }
+  for (int u = 0; u < 16 / per; ++u) {
+    const int4 w = q[u];
+    memcpy(&v[u * per], &w, 16);
   }
-#pragma unroll
-  for (int j = 0; j < 32; ++j)
-    if (i < pb && j <= i) S[(c0 + j) * LD + c0 + i] = a[j];
-  __syncwarp();
-  return fail;
 }
 
-// Rows [r0, r1) of sub-block column c0: solve x L_pp^H = b in place, one thread per
-// row, unrolled forward substitution (L read from shared memory by broadcast):
-//   x_j = (b_j - sum_{k<j} x_k conj(L(j,k))) conj(1/L(j,j)).
+// Right-looking Cholesky of the sub-panel S(c0:jb, c0:c0+pb) (pb <= 32, jb - c0 <=
+// 128), lower part, in place, by all 256 threads of the block (every thread must
+// call it).  Thread t holds row c0 + (t & 127), columns c0 + 16 (t >> 7) + q
+// (q = 0..15), in registers.  Step k:
+//   d = A(k,k), r = 1/sqrt(d)             (every thread, from the published column)
+//   L(i,k) = A(i,k) r                      (the owners of column k keep it)
+//   A(i,j) -= (L(i,k) r) conj(A(j,k)), j > k
+// and the owners of column k+1 publish it (rows k+1 ..) for the next step, so each
+// step takes one barrier.  The steps of one 16-column half are unrolled (column k
+// is register kq = k mod 16 of its owners, a compile-time index); the two halves
+// are a loop.  Elements above the diagonal and rows past jb are computed on but
+// never stored.  cbuf: 2 x 128 elements.  rdiag[c0+k] = 1/L(k,k).  Returns the
+// first failing local column (pivot <= 0 or NaN) or -1, the same in every thread;
+// on failure the columns before it are factored and the rest is left as updated.
+// Ends with a barrier.
 template <typename T, int NT>
-__device__ __noinline__ void rows_solve(T* S, int LD, int c0, int pb, int r0, int r1, const T* rdiag) {
-  for (int r = r0 + threadIdx.x; r < r1; r += NT) {
-    T x[32];
+__device__ __noinline__ int subpanel_chol(T* S, int LD, int c0, int pb, int jb, T* rdiag, T* cbuf) {
+  static_assert(NT == 256, "one thread per (row, 16-column half) of a 128 x 32 sub-panel");
+  using R = RealOf<T>;
+  const int t = threadIdx.x;
+  const int ii = t & 127;                 // local row
+  const int h = t >> 7;                   // column half
+  const bool row_ok = c0 + ii < jb;
+  T x[16];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = (j < pb) ? S[(c0 + j) * LD + r] : zero<T>();
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      if (j < pb) {
-        T s0 = x[j], s1 = zero<T>();
-#pragma unroll
-        for (int k = 0; k < j; ++k) {
-          const T l = cj(S[(c0 + k) * LD + c0 + j]);
-          if (k & 1) mac(s1, neg(x[k]), l); else mac(s0, neg(x[k]), l);
-        }
-        x[j] = mul(add(s0, s1), cj(rdiag[c0 + j]));
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 32; ++j)
-      if (j < pb) S[(c0 + j) * LD + r] = x[j];
+  for (int q = 0; q < 16; ++q) {
+    const int j = 16 * h + q;
+    x[q] = (row_ok && j < pb && ii >= j) ? S[(c0 + j) * LD + c0 + ii] : zero<T>();
   }
+  if (h == 0 && row_ok) cbuf[ii] = x[0];
+  __syncthreads();
+  int fail = -1;
+#pragma unroll 1
+  for (int kk = 0; kk < 2 && 16 * kk < pb; ++kk) {
+#pragma unroll
+    for (int kq = 0; kq < 16; ++kq) {
+      const int k = 16 * kk + kq;
+      if (k >= pb) break;                 // the same in every thread
+      const T* cur = cbuf + (k & 1) * 128;
+      T* nxt = cbuf + ((k + 1) & 1) * 128;
+      const R d = re(cur[k]);
+      if (!(d > R(0))) {
+        fail = k;
+        break;
+      }
+      const R r = rsqrt_(d);
+      const T li = (ii == k) ? from_real<T>(d * r) : scale(cur[ii], r);
+      if (h == kk && ii >= k) x[kq] = li;
+      if (t == 0) rdiag[c0 + k] = from_real<T>(r);
+      const T lir = neg(scale(li, r));
+      if (h == kk) {
+        T v[16];
+        load16(cur + 16 * kk, v);
+#pragma unroll
+        for (int q = kq + 1; q < 16; ++q) mac(x[q], lir, cj(v[q]));
+      } else if (h > kk) {
+        T v[16];
+        load16(cur + 16, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) mac(x[q], lir, cj(v[q]));
+      }
+      if (k + 1 < pb && row_ok && ii >= k + 1) {
+        if (kq < 15) {
+          if (h == kk) nxt[ii] = x[kq + 1];
+        } else if (h == kk + 1) {
+          nxt[ii] = x[0];
+        }
+      }
+      __syncthreads();
+    }
+    if (fail >= 0) break;
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int j = 16 * h + q;
+    if (row_ok && j < pb && ii >= j) S[(c0 + j) * LD + c0 + ii] = x[q];
+  }
+  __syncthreads();
+  return fail;
 }
 
 // Warp: X = inv(L_pp) for the pb x pb lower sub-block at (c0, c0) (unit: implicit
@@ -300,6 +330,7 @@ __device__ __forceinline__ void diag_factor_block(T* __restrict__ A, long long r
   T* X = reinterpret_cast<T*>(smem_raw + L::S);
   T* TMP = reinterpret_cast<T*>(smem_raw + L::S + L::X);
   T* rdiag = reinterpret_cast<T*>(smem_raw + L::S + L::X + L::TMP);
+  T* cbuf = reinterpret_cast<T*>(smem_raw + L::S + L::X + L::TMP + L::R);
   __shared__ int s_fail;
   const int tid = threadIdx.x;
   const bool rows_fast = (rs == 1);
@@ -320,15 +351,11 @@ __device__ __forceinline__ void diag_factor_block(T* __restrict__ A, long long r
       block_update<T, NT>(S, LD, c0, pb, jb);
       __syncthreads();
     }
-    if (tid < 32) {
-      const int f = warp_chol32<T>(S, LD, c0, pb, rdiag);
-      if (f >= 0 && tid == 0) s_fail = c0 + f;
-    }
-    __syncthreads();
-    if (s_fail >= 0) break;
-    if (c0 + pb < jb) {
-      rows_solve<T, NT>(S, LD, c0, pb, c0 + pb, jb, rdiag);
+    const int f = subpanel_chol<T, NT>(S, LD, c0, pb, jb, rdiag, cbuf);
+    if (f >= 0) {
+      if (tid == 0) s_fail = c0 + f;
       __syncthreads();
+      break;
     }
   }
 

@@ -1,9 +1,10 @@
 """Host-memory routines cuMultiGPU?potrf / ?trtri / ?lauum / ?potri (reference
 include/lapack.h:117-158; tests modelled on test/lapack/cumultigpu?potrf.c:40-90):
 the matrix lives in host memory, the result must equal the oracle within the
-contract's bounds and equal, bit for bit, the single-GPU routine on the same
-values; the other triangle and the padding rows stay untouched; numerical failure
-returns CUDA_ERROR_INVALID_VALUE with the oracle's info."""
+contract's bounds and, while the factorization runs as one panel (n < 2048), equal
+bit for bit the single-GPU routine on the same values; the other triangle and the
+padding rows stay untouched; numerical failure returns CUDA_ERROR_INVALID_VALUE
+with the oracle's info."""
 from __future__ import annotations
 
 import numpy as np
@@ -180,3 +181,42 @@ def test_device_list_and_sync(hosth):
     hh.close()
     m.close()
     assert hosth.synchronize() == 0
+
+
+def _pinned_colmajor(A):
+    import torch
+    lda, n = A.shape
+    P = torch.empty((n, lda), dtype=getattr(torch, str(A.dtype)), pin_memory=True)
+    P.copy_(torch.from_numpy(np.ascontiguousarray(A.T)))
+    return P
+
+
+@pytest.mark.parametrize("p", list("dz"))
+@pytest.mark.parametrize("u", ["L", "U"])
+def test_host_streamed_tall_panels(hosth, p, u):
+    """Page-locked A with n > 2048: copied in as tall panels (1024 columns up to the
+    middle column, then the rest) and factored left-looking panel by panel.  The
+    factor meets the backward-error bound; the other triangle and the padding are
+    untouched; a failure in a later panel reports its global position."""
+    n, lda = 4500, 4502
+    A = matgen.spd(p, n, seed=11, lda=lda)
+    P = _pinned_colmajor(A)
+    _, h2d0, d2h0 = hosth.stats()
+    rc, info = cc.call_host(hosth, p.upper(), "potrf", u, n, P.data_ptr(), lda)
+    assert rc == 0 and info == 0
+    _, h2d1, d2h1 = hosth.stats()
+    H = np.asfortranarray(P.numpy().T)
+    assert matgen.backward_error(A, H, u) <= 10
+    assert np.array_equal(H[:n, :n][_other(n, u)], A[:n, :n][_other(n, u)])
+    assert np.array_equal(H[n:, :], A[n:, :])
+    esz = A.itemsize
+    tri = esz * n * (n + 1) // 2
+    assert tri <= h2d1 - h2d0 <= tri + esz * n * 256
+    assert tri <= d2h1 - d2h0 <= tri + esz * n * 128
+    # not positive definite at 3001 (inside the last panel) and at 1500 (second panel)
+    for bad in (3000, 1500):
+        B = A.copy(order="F")
+        B[bad, bad] = -1.0
+        Q = _pinned_colmajor(B)
+        rc, info = cc.call_host(hosth, p.upper(), "potrf", u, n, Q.data_ptr(), lda)
+        assert rc == cc.CUDA_ERROR_INVALID_VALUE and info == bad + 1, (bad, rc, info)
