@@ -15,15 +15,22 @@
 // ?potrf with page-locked (or device) memory overlaps both copies with the
 // factorization.  Copy back: each block column of the factor is queued on an
 // outbound copy stream behind the work that finishes it.  Copy in: the matrix is
-// cut into tall panels (1024 columns wide up to the middle column, then the rest in
-// one), copied in that order, and factored left-looking panel by panel as they
-// land: a panel first receives the updates of every column left of it in one GEMM
-// (K = its first column), then potrf_run factors it as a tall panel (right-looking
-// inside, trailing updates restricted to its own columns).  The first panels hold
-// most of the bytes and little of the work, so the work waiting for the last copy
-// is the right-looking factorization of the second half.  Pageable memory is
-// copied in before and back after the driver (a copy to pageable memory returns
-// only when it is done, which would stall the queueing of the schedule).
+// cut into tall panels (1024 columns wide up to the middle column, then the second
+// half in one), copied in that order and factored left-looking panel by panel as
+// they land:
+//   * a tall panel receives the updates of the columns left of its predecessor on a
+//     background stream while the predecessor is factored, then the updates of the
+//     predecessor's columns, then potrf_run factors it (right-looking inside,
+//     trailing updates restricted to its own columns);
+//   * the last panel receives the updates of each tall panel as soon as that panel
+//     is factored and the last panel has landed, on a lowest-priority stream: this
+//     bulk of the work fills the SMs that the latency-bound tall-panel
+//     factorizations leave idle;
+//   * then potrf_run factors the last panel right-looking.
+// Background updates run in launches of at most 1024 columns of K, so the panel
+// stream's one-CTA kernels wait little for an SM.  Pageable memory is copied in
+// before and back after the driver (a copy to pageable memory returns only when it
+// is done, which would stall the queueing of the schedule).
 // A call returns when its copies have landed.  The device buffer is cached in the
 // handle (grow-only, leading dimension rounded up to 32 elements).
 #pragma once
@@ -58,7 +65,9 @@ struct __cumultigpulapackhandle_st {
                                     // routines that do not overlap them)
   cudaStream_t s_out = nullptr;     // device -> host copies overlapped with ?potrf
   cudaEvent_t ev = nullptr;
-  cudaStream_t s_gemm = nullptr;    // ?potrf: updates of the next tall panel (low priority)
+  cudaStream_t s_gemm = nullptr;    // ?potrf: updates of the next tall panel
+  cudaStream_t s_tail = nullptr;    // ?potrf: updates of the last panel (low priority)
+  cudaEvent_t ev_tail = nullptr;
   std::vector<cudaEvent_t> ev_in;   // one per tall panel copied in
   std::vector<cudaEvent_t> ev_a;    // one per tall panel: its early updates are done
   void* buf = nullptr;              // staged matrix (grow-only)
@@ -143,10 +152,12 @@ inline CUresult finish(CUmultiGPULAPACKhandle hh, CUresult r) {
   cudaError_t e = cudaStreamSynchronize(hh->s_copy);
   cudaError_t e2 = cudaStreamSynchronize(hh->s_out);
   cudaError_t e3 = cudaStreamSynchronize(hh->s_gemm);
+  cudaError_t e4 = cudaStreamSynchronize(hh->s_tail);
   if (r != CUDA_SUCCESS) return r;
   CUCHOL_CHECK(e);
   CUCHOL_CHECK(e2);
   CUCHOL_CHECK(e3);
+  CUCHOL_CHECK(e4);
   return CUDA_SUCCESS;
 }
 
@@ -207,34 +218,51 @@ CUresult host_potrf_run(CUmultiGPULAPACKhandle hh, bool upper, size_t n, T* A, s
   }
   const T minus_one = from_real<T>(RealOf<T>(-1)), one = from_real<T>(RealOf<T>(1));
   // A(c0:, c0:c0+w) -= L(c0:, k0:k1) L(c0:c0+w, k0:k1)^H, lower-only on the panel's
-  // diagonal block
+  // diagonal block, in launches of at most 1024 columns of L each: a tile of a
+  // background launch then holds its SM for a fraction of a millisecond, so the
+  // panel stream's one-CTA kernels find a free SM soon after they are queued.
   auto catch_up = [&](size_t c0, size_t w, size_t k0, size_t k1, cudaStream_t s) -> CUresult {
-    if (k1 <= k0) return CUDA_SUCCESS;
-    GemmProblem<T> u = problem<T>();
-    u.a = at(c0, k0); u.a_rs = rs; u.a_ks = cs;
-    u.b = at(c0, k0); u.b_rs = rs; u.b_ks = cs; u.conj_b = 1;
-    u.c = at(c0, c0); u.c_rs = rs; u.c_cs = cs;
-    u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
-    u.alpha = minus_one; u.beta = one;
-    u.lower_only = 1; u.real_diag = 1;
-    u.m = (int)(n - c0); u.n = (int)w; u.k = (int)(k1 - k0);
-    return gemm<T>(h, u, s, nullptr);
+    for (size_t k = k0; k < k1; k += kPanelCols) {
+      GemmProblem<T> u = problem<T>();
+      u.a = at(c0, k); u.a_rs = rs; u.a_ks = cs;
+      u.b = at(c0, k); u.b_rs = rs; u.b_ks = cs; u.conj_b = 1;
+      u.c = at(c0, c0); u.c_rs = rs; u.c_cs = cs;
+      u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
+      u.alpha = minus_one; u.beta = one;
+      u.lower_only = 1; u.real_diag = 1;
+      u.m = (int)(n - c0); u.n = (int)w; u.k = (int)std::min(kPanelCols, k1 - k);
+      CUCHOL_CHECK_CU(gemm<T>(h, u, s, nullptr));
+    }
+    return CUDA_SUCCESS;
   };
-  // Panel r receives the updates of columns 0 .. plan[r-1]-1 on the low-priority
-  // stream while panel r-1 is factored (those columns are final by then), and the
-  // updates of panel r-1's columns on the panel stream after it.
+  // A tall panel r receives the updates of columns 0 .. plan[r-1]-1 in one GEMM on a
+  // low-priority stream while panel r-1 is factored (those columns are final by
+  // then), and the updates of panel r-1's columns on the panel stream after it.  The
+  // last panel (the second half) takes the updates of each tall panel as soon as that
+  // panel is factored and the last panel has landed, on a second low-priority stream,
+  // so they fill the GPU around the latency-bound tall-panel factorizations.
+  const size_t last = panels - 1;
   for (size_t r = 0; r < panels; ++r) {
     const size_t c0 = plan[r], w = plan[r + 1] - c0;
     CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_in[r], 0));
     CUCHOL_CHECK(cudaStreamWaitEvent(h->s_update, hh->ev_in[r], 0));
     if (r >= 1) {
-      if (r >= 2) CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_a[r], 0));
+      if (r == last) {
+        if (r >= 2) CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_tail, 0));
+      } else if (r >= 2) {
+        CUCHOL_CHECK(cudaStreamWaitEvent(h->s_panel, hh->ev_a[r], 0));
+      }
       CUCHOL_CHECK_CU(catch_up(c0, w, plan[r - 1], c0, h->s_panel));
     }
-    if (r + 1 < panels && r >= 1) {
+    if (r >= 1 && r + 1 < last) {
       CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_gemm, hh->ev_in[r + 1], 0));
       CUCHOL_CHECK_CU(catch_up(plan[r + 1], plan[r + 2] - plan[r + 1], 0, c0, hh->s_gemm));
       CUCHOL_CHECK(cudaEventRecord(hh->ev_a[r + 1], hh->s_gemm));
+    }
+    if (r >= 1 && r < last) {
+      if (r == 1) CUCHOL_CHECK(cudaStreamWaitEvent(hh->s_tail, hh->ev_in[last], 0));
+      CUCHOL_CHECK_CU(catch_up(plan[last], n - plan[last], plan[r - 1], c0, hh->s_tail));
+      CUCHOL_CHECK(cudaEventRecord(hh->ev_tail, hh->s_tail));
     }
     FinalColumns back = [&](int c, int jb, cudaStream_t s) -> CUresult {
       CUCHOL_CHECK(cudaEventRecord(hh->ev, s));
@@ -375,11 +403,18 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKCreate(CUmultiGPULAPACKhandle*
   if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithFlags(&hh->s_out, cudaStreamNonBlocking));
   int lo = 0, hi = 0;
   if (r == CUDA_SUCCESS) r = to_cu(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithPriority(&hh->s_gemm, cudaStreamNonBlocking, lo));
+  // the next panel's updates (on the panel chain) rank with the factorization's own
+  // trailing updates; the last panel's updates only fill SMs left idle
+  const int mid = (hi < lo - 1) ? (lo + hi) / 2 : lo;
+  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithPriority(&hh->s_gemm, cudaStreamNonBlocking, mid));
+  if (r == CUDA_SUCCESS) r = to_cu(cudaStreamCreateWithPriority(&hh->s_tail, cudaStreamNonBlocking, lo));
+  if (r == CUDA_SUCCESS) r = to_cu(cudaEventCreateWithFlags(&hh->ev_tail, cudaEventDisableTiming));
   if (r == CUDA_SUCCESS) r = to_cu(cudaEventCreateWithFlags(&hh->ev, cudaEventDisableTiming));
   if (r != CUDA_SUCCESS) {
     if (hh->ev) cudaEventDestroy(hh->ev);
     if (hh->s_out) cudaStreamDestroy(hh->s_out);
+    if (hh->ev_tail) cudaEventDestroy(hh->ev_tail);
+    if (hh->s_tail) cudaStreamDestroy(hh->s_tail);
     if (hh->s_gemm) cudaStreamDestroy(hh->s_gemm);
     if (hh->s_copy) cudaStreamDestroy(hh->s_copy);
     if (hh->h) cuLAPACKDestroy(hh->h);
@@ -397,8 +432,11 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKDestroy(CUmultiGPULAPACKhandle
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_out));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_gemm));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_tail));
   if (hh->buf) cudaFree(hh->buf);
   cudaEventDestroy(hh->ev);
+  cudaEventDestroy(hh->ev_tail);
+  cudaStreamDestroy(hh->s_tail);
   for (cudaEvent_t e : hh->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : hh->ev_a) cudaEventDestroy(e);
   cudaStreamDestroy(hh->s_gemm);
@@ -416,6 +454,7 @@ extern "C" CUCHOL_EXPORT CUresult cuMultiGPULAPACKSynchronize(CUmultiGPULAPACKha
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_copy));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_out));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->s_gemm));
+  CUCHOL_CHECK(cudaStreamSynchronize(hh->s_tail));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_panel));
   CUCHOL_CHECK(cudaStreamSynchronize(hh->h->s_update));
   return CUDA_SUCCESS;

@@ -616,9 +616,13 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   CUCHOL_CHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
   int lo = 0, hi = 0;
   CUCHOL_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-  // blocking streams: they order after work the caller queued on the legacy stream
+  // blocking streams: they order after work the caller queued on the legacy stream.
+  // The update stream sits between the panel stream and the lowest priority, which
+  // is left for background work queued next to a factorization (the host-memory
+  // ?potrf's updates of panels further right).
+  const int mid = (hi < lo - 1) ? (lo + hi) / 2 : lo;
   CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_panel, cudaStreamDefault, hi));
-  CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_update, cudaStreamDefault, lo));
+  CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_update, cudaStreamDefault, mid));
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_panel, cudaEventDisableTiming));
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_update, cudaEventDisableTiming));
   CUCHOL_CHECK(cudaMalloc(&h->d_words, 16 * sizeof(int)));
