@@ -107,7 +107,7 @@ CUresult cuZlogdet(CULAPACKhandle, CUdeviceptr, size_t, size_t, double *, CUstre
  * the rest of the factorization runs.  Same argument checks as the reference
  * (lda < n: info -4, -5 for ?trtri); numerical failure (info > 0) returns
  * CUDA_ERROR_INVALID_VALUE as the reference's host-memory routines do
- * (lapack/dpotrf.c:331, lapack/dtrtri.c:498, lapack/dpotri.c:64), and a singular
+ * (lapack/dpotrf.c:330, lapack/dtrtri.c:499, lapack/dpotri.c:64), and a singular
  * ?trtri leaves A unmodified.  The handle caches one device buffer of the largest
  * matrix seen; calls on one handle must not overlap. */
 typedef struct __cumultigpulapackhandle_st * CUmultiGPULAPACKhandle;
