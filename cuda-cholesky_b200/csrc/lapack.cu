@@ -964,3 +964,4 @@ CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 #include "mixed.cuh"
 #include "ozaki_driver.cuh"
 #include "hostmem.cuh"
+#include "rng.cuh"

@@ -87,7 +87,11 @@ def extension_symbols() -> list[str]:
               "cuCholBatchedResults", "cuCholBatchedGetBlockSize", "cuCholBatchedDestroy", "cuDlogdetNoAlloc",
               "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
               "cuCholMixedGetFactor", "cuSsyrkLowp", "cuDpotrfOzaki",
-              "cuCholMixedDestroy", "cuDposvMixed", "cuMultiGPULAPACKGetStats"]
+              "cuCholMixedDestroy", "cuDposvMixed", "cuMultiGPULAPACKGetStats", "cuSlatmc", "cuDlatmc", "cuClatmc",
+              "cuZlatmc", "philox32_t", "philox64_t"]
+    for b in ("32", "64"):
+        names += [f"cuRng{b}{f}" for f in ("Create", "Destroy", "Set", "Get", "GetOpenOpen", "GetOpenClose",
+                                           "GetCloseOpen", "GetCloseClose")]
     return names
 
 
@@ -629,3 +633,67 @@ def call_host(hh, prefix: str, routine: str, uplo: str, n: int, ptr: int, lda: i
     else:
         rc = f(h, _uplo(uplo), n, ptr, lda, C.byref(info))
     return rc, info.value
+
+
+# ---- device RNG (include/curng.h) and the SPD generator cu?latmc -----------------
+
+_RNG_FILL = {"raw": "Get", "oo": "GetOpenOpen", "oc": "GetOpenClose", "co": "GetCloseOpen", "cc": "GetCloseClose"}
+
+
+class Rng:
+    """CUrng32 (bits=32) or CUrng64 (bits=64) of the Philox4x32-10 type."""
+
+    def __init__(self, bits: int = 64, seed: int | None = None):
+        L = lib()
+        self.bits = bits
+        self._p = f"cuRng{bits}"
+        self._g = C.c_void_p()
+        typ = C.c_void_p.in_dll(L, "philox32_t" if bits == 32 else "philox64_t")
+        f = getattr(L, self._p + "Create")
+        f.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
+        f.restype = C.c_int
+        rc = f(C.byref(self._g), typ)
+        if rc != CUDA_SUCCESS:
+            raise CuCholeskyError(self._p + "Create", rc)
+        if seed is not None:
+            self.set(seed)
+
+    @property
+    def value(self) -> C.c_void_p:
+        return self._g
+
+    def set(self, seed: int) -> int:
+        f = getattr(lib(), self._p + "Set")
+        f.argtypes = [C.c_void_p, C.c_uint32 if self.bits == 32 else C.c_uint64]
+        f.restype = C.c_int
+        return f(self._g, seed)
+
+    def fill(self, ptr: int, n: int, kind: str = "raw") -> int:
+        """cuRng{32,64}{Get, GetOpenOpen, ...} into device memory at ptr (legacy stream)."""
+        f = getattr(lib(), self._p + _RNG_FILL[kind])
+        f.argtypes = [C.c_void_p, C.c_uint64, C.c_size_t]
+        f.restype = C.c_int
+        return f(self._g, ptr, n)
+
+    def close(self) -> None:
+        if self._g:
+            f = getattr(lib(), self._p + "Destroy")
+            f.argtypes = [C.c_void_p]
+            f(self._g)
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def call_latmc(prefix: str, rng, n: int, c: float, ptr: int, lda: int, stream: int = 0) -> int:
+    """cu{S,D,C,Z}latmc: Hermitian positive definite n x n matrix with condition number
+    c from the generator's stream (rng=None exercises the argument checks)."""
+    f = getattr(lib(), f"cu{prefix}latmc")
+    f.argtypes = [C.c_void_p, C.c_size_t, C.c_float if prefix in "SC" else C.c_double, C.c_uint64, C.c_size_t,
+                  C.c_void_p]
+    f.restype = C.c_int
+    return f(rng.value if rng is not None else None, n, c, ptr, lda, C.c_void_p(stream))

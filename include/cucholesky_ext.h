@@ -7,6 +7,7 @@
 #define CUCHOLESKY_EXT_H
 
 #include "lapack.h"
+#include "curng.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -137,6 +138,21 @@ CUresult cuSsyrkLowp(CULAPACKhandle, int, size_t, size_t, float, CUdeviceptr, si
  * products are exact INT32 sums, and only the final FP64 combination rounds (7 or 8
  * slices: FP64-level backward error).  No counterpart in the reference library. */
 CUresult cuDpotrfOzaki(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, int, long *);
+
+/* Random Hermitian positive definite n x n matrix with condition number c, on the
+ * device, from the generator's stream (the reference's test generator ?latmc,
+ * test/lapack/util/dlatmc.c:11-70, zlatmc.c): D = diag(1, c, d_2 .. d_{n-1}) with d_j
+ * uniform in [1, c], u uniform in [0,1] (complex: both parts), and
+ * A = H D H^H for the Householder reflection H = I - 2 u u^H / u^H u, so the
+ * eigenvalues of A are exactly D's.  Draws, in order, with the generator's [0,1]
+ * conversion: d_2 .. d_{n-1}, then u (complex: real and imaginary part of each
+ * element in turn).  The full matrix is written (exactly Hermitian); the padding rows
+ * are not touched.  Queued on `stream`.  n < 2, c < 1 or lda < n: XERBLA with the
+ * position (2, 3, 5) and CUDA_ERROR_INVALID_VALUE. */
+CUresult cuSlatmc(CUrng32, size_t, float, CUdeviceptr, size_t, CUstream);
+CUresult cuDlatmc(CUrng64, size_t, double, CUdeviceptr, size_t, CUstream);
+CUresult cuClatmc(CUrng32, size_t, float, CUdeviceptr, size_t, CUstream);
+CUresult cuZlatmc(CUrng64, size_t, double, CUdeviceptr, size_t, CUstream);
 
 /* Counters of a host-memory handle since its creation (for measurement): kernels
  * launched, and bytes copied host -> device and device -> host.  Any pointer may be

@@ -199,3 +199,38 @@ def test_headers_compile(tmp_path, lang):
     r = subprocess.run([cc_, *std, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
                         "-c", str(src), "-o", str(tmp_path / "h.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_rng_and_latmc_argument_errors():
+    """cu?latmc checks n (position 2), c (3) and lda (5) before any device work; an
+    unknown generator type or a NULL generator is CUDA_ERROR_INVALID_VALUE."""
+    lib = cucholesky.lib()
+    calls = []
+    XERBLA = C.CFUNCTYPE(None, C.c_char_p, C.c_long)
+
+    def hook(name, info):
+        calls.append((name.decode(), info))
+
+    cb = XERBLA(hook)
+    xer = C.c_void_p.in_dll(lib, "xerbla")
+    old = xer.value
+    xer.value = C.cast(cb, C.c_void_p).value
+    try:
+        for p in "SDCZ":
+            for (n, c, lda), pos in (((1, 10.0, 1), 2), ((10, 0.5, 10), 3), ((10, 10.0, 9), 5)):
+                assert cucholesky.call_latmc(p, None, n, c, 0, lda) == cucholesky.CUDA_ERROR_INVALID_VALUE
+                assert calls[-1] == (f"cu{p}latmc", pos)
+            n_calls = len(calls)
+            assert cucholesky.call_latmc(p, None, 10, 10.0, 0, 10) == cucholesky.CUDA_ERROR_INVALID_VALUE
+            assert len(calls) == n_calls
+    finally:
+        xer.value = old
+    for b in ("32", "64"):
+        f = getattr(lib, f"cuRng{b}Create")
+        f.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
+        g = C.c_void_p()
+        assert f(C.byref(g), None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert f(None, C.c_void_p.in_dll(lib, f"philox{b}_t")) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        d = getattr(lib, f"cuRng{b}Destroy")
+        d.argtypes = [C.c_void_p]
+        assert d(None) == cucholesky.CUDA_ERROR_INVALID_VALUE

@@ -135,3 +135,19 @@ def test_info_nan_and_zero_pivots():
 def test_argument_errors():
     A = np.asfortranarray(np.eye(4))
     assert O.potrf("d", "L", A, lda=3) == -4
+
+
+def test_philox_known_answers():
+    """The host Philox4x32-10 against the published known-answer vectors of the
+    generator (Random123 kat_vectors: zero, all-ones and pi-digit inputs)."""
+    import numpy as np
+    import philox_ref as P
+    cases = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in cases:
+        got = P.philox4x32_10(np.array([ctr], dtype=np.uint64), key)[0]
+        assert [int(v) for v in got] == list(want), (ctr, key, [hex(int(v)) for v in got])
