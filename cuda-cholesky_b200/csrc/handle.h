@@ -28,6 +28,7 @@ struct __culapackhandle_st {
   int num_sms;
   unsigned long long launches;   // kernels launched by this handle
   int force_simt;                // testing: route FP64 products to the SIMT engine
+  int potrf_sub;                 // ?potrf outer block in diagonal blocks (0: tuning table)
 };
 
 namespace cuchol {

@@ -19,6 +19,7 @@
 #include "handle.h"
 #include "panel.cuh"
 #include "trsm.cuh"
+#include "tuning.cuh"
 
 using namespace cuchol;
 
@@ -78,8 +79,13 @@ namespace {
 
 __global__ void narrow_double_kernel(const double* s, float* d) { *d = (float)*s; }
 
-template <typename T> struct Tune { static constexpr int nb = 128; };
+template <typename T> struct Tune { static constexpr int nb = 128; };   // diagonal block
 template <> struct Tune<cuDoubleComplex> { static constexpr int nb = 64; };
+
+template <typename T> constexpr char type_char() {
+  return std::is_same<T, float>::value ? 'S' : std::is_same<T, double>::value ? 'D'
+       : std::is_same<T, cuFloatComplex>::value ? 'C' : 'Z';
+}
 
 inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -289,18 +295,20 @@ CUresult set_smem(const void* fn, size_t bytes) {
 }
 
 // ---- ?POTRF ---------------------------------------------------------------------
-// Right-looking blocked Cholesky, outer blocks of 2*nb columns (each factored as two
-// nb-wide sub-panels), lookahead depth 1, on two streams:
-//   panel stream : for each sub-panel: diagonal-block factor + inverse W (one CTA)
-//                  -> panel solve P = A21 W^H (tensor-core GEMM into the packed
-//                  buffer P); between the two sub-panels, the update of the second
-//                  one by the first.  Then [wait previous trailing update] -> update
-//                  of the next outer block (lookahead, k = 2*nb)
-//   update stream: [wait panel] -> copy P into A -> update of the rest of the
-//                  trailing matrix (k = 2*nb)
+// Right-looking blocked Cholesky, outer blocks of NB = sub*nb columns (each factored
+// as sub nb-wide sub-panels; sub from the tuning table, 2 to 8 by n for FP64),
+// lookahead depth 1, on two streams:
+//   panel stream : for each sub-panel: diagonal-block factor (+ inverse W for complex
+//                  types) -> panel solve into the packed buffer P -> the update of the
+//                  outer block's remaining sub-panel columns by it.  Then [wait
+//                  previous trailing update] -> update of the next outer block
+//                  (lookahead, k = NB)
+//   update stream: [wait panel] -> (complex: copy P into A) -> update of the rest of
+//                  the trailing matrix (k = NB)
 // The next outer block is factored on a few SMs while the trailing update of the
-// previous one runs on the rest; the wide outer block halves the number of
-// trailing-update tiles per flop (their fill and drain are the engine's overhead).
+// previous one runs on the rest; a wider outer block cuts the trailing update's
+// tiles per flop (their fill and drain are the engine's overhead) at the price of
+// more panel-stream work per step, so the best width grows with n.
 // P (ping-pong pair) holds rows from the first sub-panel's diagonal block down:
 // P(r, c) = L(j + nb + r, j + c).  Failure: the diagonal kernel sets the device
 // info word, and every later kernel exits at entry when it is set.
@@ -320,7 +328,8 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
                    const FinalColumns* on_final = nullptr, int ncols = -1) {
   if (ncols < 0 || ncols > n) ncols = n;
   constexpr int nb = Tune<T>::nb;
-  constexpr int NB = 2 * nb;
+  // outer block: sub diagonal blocks, from the handle's override or the tuning table
+  const int NB = (h->potrf_sub > 0 ? h->potrf_sub : tuned_potrf_sub(type_char<T>(), n)) * nb;
   using Smem = DiagSmem<T, nb>;
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
   auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
@@ -400,16 +409,17 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
         CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
         if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, su));
       }
-      if (s0 == 0 && jB > nb) {
-        // the second sub-panel's columns (rows j + nb ..) by the first sub-panel
-        CUCHOL_CHECK_CU(update(j + nb, j + nb, n - j - nb, jB - nb, P, P, nb, sp));
+      if (s0 + nb < jB) {
+        // the outer block's remaining sub-panel columns (rows c + nb ..) by this one
+        const T* Pc = P + s0 + (long long)s0 * ldp;
+        CUCHOL_CHECK_CU(update(c + nb, c + nb, n - c - nb, jB - s0 - nb, Pc, Pc, nb, sp));
       }
     }
     if (m == 0 || mc == 0) break;
     // lookahead: next outer block (P rows from j + NB, k = jB), after the previous
     // trailing update
     const int jB2 = std::min(NB, mc);
-    const T* Pt = P + nb;
+    const T* Pt = P + (NB - nb);
     CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
     CUCHOL_CHECK_CU(update(j + NB, j + NB, m, jB2, Pt, Pt, jB, sp));
     // rest of the trailing matrix, once P holds both sub-panels
@@ -613,6 +623,15 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
     const char* e = getenv("CUCHOLESKY_FORCE_SIMT");   // testing: FP64 products on the SIMT engine
     h->force_simt = (e != nullptr && e[0] == '1') ? 1 : 0;
   }
+  {
+    // a tuning file named by the environment replaces the built-in table once
+    static std::once_flag once;
+    std::call_once(once, [] {
+      const char* path = getenv("CUCHOLESKY_TUNING");
+      if (path != nullptr && path[0] != '\0' && !load_tuning(path))
+        fprintf(stderr, "cucholesky: tuning file %s not loaded (unreadable or malformed)\n", path);
+    });
+  }
   CUCHOL_CHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
   int lo = 0, hi = 0;
   CUCHOL_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -809,6 +828,24 @@ CUCHOL_API_LOGDET(Z, cuDoubleComplex)
 extern "C" CUCHOL_EXPORT CUresult cuLAPACKGetLaunchCount(CULAPACKhandle h, unsigned long long* count) {
   if (h == nullptr || count == nullptr) return CUDA_ERROR_INVALID_VALUE;
   *count = h->launches;
+  return CUDA_SUCCESS;
+}
+
+// ---- tuning table (tuning.cuh) -------------------------------------------------------
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKLoadTuning(const char* path) {
+  if (path == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  return load_tuning(path) ? CUDA_SUCCESS : CUDA_ERROR_INVALID_VALUE;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKSetPotrfBlocks(CULAPACKhandle h, int sub) {
+  if (h == nullptr || sub < 0 || sub > kMaxSub) return CUDA_ERROR_INVALID_VALUE;
+  h->potrf_sub = sub;
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKGetPotrfBlocks(CULAPACKhandle h, char type, size_t n, int* sub) {
+  if (sub == nullptr || strchr("SDCZ", type) == nullptr || type == '\0') return CUDA_ERROR_INVALID_VALUE;
+  *sub = (h != nullptr && h->potrf_sub > 0) ? h->potrf_sub : tuned_potrf_sub(type, (long long)n);
   return CUDA_SUCCESS;
 }
 

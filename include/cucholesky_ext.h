@@ -25,6 +25,21 @@ CUresult cuCpotrfLogdet(CULAPACKhandle, CBlasUplo, size_t, CUdeviceptr, size_t, 
  * measurement; counts this library's own kernels only). */
 CUresult cuLAPACKGetLaunchCount(CULAPACKhandle, unsigned long long *);
 
+/* Tuning table (the counterpart of the reference's build-time include/config.h,
+ * written by its blas/config.c): process-wide rows "potrf <S|D|C|Z> <n_min> <sub>"
+ * choosing ?potrf's outer block (sub diagonal blocks of 128 columns, 64 for Z) for
+ * orders n >= n_min.  Built-in rows were measured on a B200; cuLAPACKLoadTuning
+ * replaces them with a file in the text format written by
+ * cuda-cholesky_b200/cucholesky/tune.py (first line "cucholesky-tuning 1"; the
+ * CUCHOLESKY_TUNING environment variable names one to load when the first handle is
+ * created).  A malformed file leaves the table unchanged and returns
+ * CUDA_ERROR_INVALID_VALUE.  cuLAPACKSetPotrfBlocks overrides the table for one handle
+ * (1..16; 0 restores the table); cuLAPACKGetPotrfBlocks reports the value ?potrf of
+ * that type and order would use (handle may be NULL: the table alone). */
+CUresult cuLAPACKLoadTuning(const char *);
+CUresult cuLAPACKSetPotrfBlocks(CULAPACKhandle, int);
+CUresult cuLAPACKGetPotrfBlocks(CULAPACKhandle, char, size_t, int *);
+
 /* Batched factor, log det and inverse of many small SPD matrices of uneven sizes
  * (each matrix b: order n[b], device pointer A[b], leading dimension lda[b], all
  * in the same `uplo` storage).  No counterpart in the reference library.

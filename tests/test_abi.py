@@ -234,3 +234,45 @@ def test_rng_and_latmc_argument_errors():
         d = getattr(lib, f"cuRng{b}Destroy")
         d.argtypes = [C.c_void_p]
         assert d(None) == cucholesky.CUDA_ERROR_INVALID_VALUE
+
+
+def test_tuning_table_file(tmp_path):
+    """The tuning table: built-in FP64 rows; a file in the tuner's format replaces
+    them; a malformed file or an unknown version is refused and changes nothing."""
+    import importlib
+    lib = cucholesky.lib()
+    tune = importlib.import_module("cucholesky.tune")
+    tune._declare(lib)
+
+    def sub(t, n):
+        v = C.c_int(0)
+        assert lib.cuLAPACKGetPotrfBlocks(None, t.encode(), n, C.byref(v)) == 0
+        return v.value
+
+    assert sub("D", 1000) == 2 and sub("D", 16384) == 4 and sub("D", 65536) == 8 and sub("Z", 65536) == 2
+    rows = tune.table_rows("D", {4096: 2, 8192: 3, 16384: 5})
+    assert rows == ["potrf D 0 2", "potrf D 5793 3", "potrf D 11585 5"]
+    good = tmp_path / "t.tuning"
+    good.write_text("cucholesky-tuning 1\n# comment\n" + "\n".join(rows) + "\npotrf S 0 3\n")
+    bad_version = tmp_path / "v.tuning"
+    bad_version.write_text("cucholesky-tuning 2\npotrf D 0 4\n")
+    bad_row = tmp_path / "r.tuning"
+    bad_row.write_text("cucholesky-tuning 1\npotrf D 0 99\n")
+    builtin = [(t, n, sub(t, n)) for t in "SDCZ" for n in (100, 7000, 20000, 70000)]
+    try:
+        assert lib.cuLAPACKLoadTuning(str(good).encode()) == 0
+        assert sub("D", 5000) == 2 and sub("D", 6000) == 3 and sub("D", 100000) == 5
+        assert sub("S", 10) == 3 and sub("Z", 10) == 2            # no row: 2
+        for f in (bad_version, bad_row, tmp_path / "missing.tuning"):
+            assert lib.cuLAPACKLoadTuning(str(f).encode()) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert sub("D", 100000) == 5
+        assert lib.cuLAPACKGetPotrfBlocks(None, b"Q", 10, C.byref(C.c_int())) == cucholesky.CUDA_ERROR_INVALID_VALUE
+        assert lib.cuLAPACKSetPotrfBlocks(None, 3) == cucholesky.CUDA_ERROR_INVALID_VALUE
+    finally:
+        restore = tmp_path / "builtin.tuning"
+        lines = ["cucholesky-tuning 1"]
+        lines += ["potrf D 0 2", "potrf D 6144 3", "potrf D 12288 4", "potrf D 24576 6", "potrf D 49152 8",
+                  "potrf S 0 2", "potrf C 0 2", "potrf Z 0 2"]
+        restore.write_text("\n".join(lines) + "\n")
+        assert lib.cuLAPACKLoadTuning(str(restore).encode()) == 0
+    assert [(t, n, sub(t, n)) for t in "SDCZ" for n in (100, 7000, 20000, 70000)] == builtin

@@ -237,3 +237,32 @@ def test_determinism(handle):
     X1, _ = gpu_call(handle, "potri", "d", "L", F1)
     X2, _ = gpu_call(handle, "potri", "d", "L", F1)
     assert np.array_equal(X1, X2)
+
+
+@pytest.mark.parametrize("p", list("dz"))
+@pytest.mark.parametrize("u", ["L", "U"])
+def test_outer_block_sizes(handle, p, u):
+    """Every ?potrf outer-block size the tuning table may choose (1..8 diagonal
+    blocks, here forced per handle) gives a factor within the bounds, on an order
+    that leaves a partial outer block; the table's own choice is restored after."""
+    import ctypes as C
+    from cucholesky import tune
+    lib = cc.lib()
+    tune._declare(lib)
+    n, lda = 1100, 1103
+    A = matgen.spd(p, n, seed=5, lda=lda)
+    Fo = A.copy(order="F")
+    assert O.potrf(p, u, Fo, lda=lda) == 0
+    try:
+        for sub in (1, 2, 3, 4, 6, 8):
+            assert lib.cuLAPACKSetPotrfBlocks(handle.value, sub) == 0
+            F, info = gpu_call(handle, "potrf", p, u, A)
+            assert info == 0
+            assert matgen.backward_error(A, F, u) <= 10, sub
+            d = np.abs(_tri(u)(F[:n, :n] - Fo[:n, :n])).max()
+            assert d <= 50 * n * EPS[p] * np.abs(A[:n, :n]).max(), (sub, d)
+    finally:
+        assert lib.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
+    v = C.c_int(0)
+    assert lib.cuLAPACKGetPotrfBlocks(handle.value, p.upper().encode(), 16384, C.byref(v)) == 0
+    assert v.value == (4 if p == "d" else 2)
