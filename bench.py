@@ -746,10 +746,15 @@ def main():
     nlaunch = launches() - l0
 
     # the dominant kernel alone: the trailing update (tensor-core SYRK) at the shape
-    # of the factorization's first outer step, m = n - 512 rows, k = 256, timed with
-    # CUDA events on the stream it is launched on
+    # of the factorization's first outer step, k = the outer block the tuning table
+    # picks for this n (sub diagonal blocks of 128), m = n - k rows, timed with CUDA
+    # events on the stream it is launched on
     bh = cc.BlasHandle()
-    mk, kk = n - 512, 256
+    sub = C.c_int(0)
+    lib.cuLAPACKGetPotrfBlocks.argtypes = [C.c_void_p, C.c_char, C.c_size_t, C.POINTER(C.c_int)]
+    assert lib.cuLAPACKGetPotrfBlocks(h.value, b"D", n, C.byref(sub)) == 0
+    kk = 128 * sub.value
+    mk = n - kk
     Pk = torch.randn(kk, mk, dtype=torch.float64, device=dev)     # column-major mk x kk
     Ck = torch.zeros(mk, mk, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream()
@@ -764,10 +769,11 @@ def main():
     syrk_ms = statistics.mean(a.elapsed_time(b) for a, b in kev)
     syrk_flops = float(mk) * (mk + 1) * kk          # lower triangle incl. diagonal
     syrk_tflops = syrk_flops / (syrk_ms / 1e3) / 1e12
-    # DRAM traffic per launch: 15.1 bytes per lower-triangle element of C, from the
-    # ncu capture of the same kernel at m = 8192, k = 256 (profiles/), scaled by the
-    # number of C elements (C's read + write dominate; the panel stays in L2)
-    syrk_traffic = 15.1 * (float(mk) * (mk + 1) / 2)
+    # DRAM traffic per launch, from the ncu captures of the same kernel at m = 8192
+    # (profiles/): bytes per lower-triangle element of C (14.6 at k = 256, 16.05 at
+    # k = 512; C's read + write) scaled by the number of C elements, plus the panel
+    # read once (8 m k bytes; it stays in L2)
+    syrk_traffic = (16.05 if kk >= 512 else 14.6) * (float(mk) * (mk + 1) / 2) + 8.0 * mk * kk
     del Pk, Ck
     bh.close()
     total_ms = t0.elapsed_time(t1)
@@ -843,7 +849,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"dpotrf {args.uplo} FP64 n={n} lda={n}, A=G*G^T/n+I, G~U[-1,1]",
-                       "n": n, "uplo": args.uplo, "lda": n, "nb": 128,
+                       "n": n, "uplo": args.uplo, "lda": n, "nb": 128, "outer_block": kk,
                        "l2": "each step restores A (2 GiB) from a pristine copy: inputs larger than L2",
                        "parallelism": "replicas" if world > 1 else "single"},
             "potrf_ms": statistics.mean(potrf_ms),
