@@ -610,19 +610,24 @@ def run_ozaki(args) -> None:
 
     Aw = torch.empty_like(A0)
     out = {}
+    # each arm twice on a fresh copy of A; the first run of each also grows the
+    # handle's workspace to its size, so the second is the one reported
     for name, call in (("native_dmma", lambda: cc.call_potrf(h, "D", "L", n, Aw.data_ptr(), n)),
                        ("ozaki_int8", lambda: ozaki(Aw.data_ptr(), n, n))):
-        Aw.copy_(A0)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        rc, info = call()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        out[name] = {"potrf_ms": ms, "tflops": n ** 3 / 3 / (ms / 1e3) / 1e12, "rc": rc, "info": info,
-                     "backward_error_n_eps_probe": factor_error(Aw)}
+        runs = []
+        for _ in range(2):
+            Aw.copy_(A0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rc, info = call()
+            e1.record()
+            torch.cuda.synchronize()
+            runs.append(e0.elapsed_time(e1))
+        ms = runs[-1]
+        out[name] = {"potrf_ms": ms, "first_run_ms": runs[0], "tflops": n ** 3 / 3 / (ms / 1e3) / 1e12, "rc": rc,
+                     "info": info, "backward_error_n_eps_probe": factor_error(Aw)}
     # the inverse from the Ozaki factor (native ?potri)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)

@@ -19,7 +19,9 @@
 // two passes, d = 2..5 and d = 6..S+1, each folded into C:
 //   * thread 0 streams the 128-row slice tiles A_t (k-major, 128-byte swizzle, one TMA
 //     box per 128 k) through a 2-stage ring and, for each u of the pass, the slice tile
-//     B_u through a 4-stage ring;
+//     B_u through a 4-stage ring; a stage holds up to 256 of k, and a longer k (the
+//     driver's 512) runs as consecutive 256-wide halves that accumulate into the same
+//     TMEM accumulators, so one epilogue per pass serves the whole k;
 //   * thread 32 issues tcgen05.mma.cta_group::1.kind::i8 (M = N = 128, K = 32) on
 //     A_t x B_u into the accumulator of its diagonal and frees the stages with
 //     tcgen05.commit;
@@ -36,7 +38,7 @@ namespace cuchol {
 namespace oz {
 
 constexpr int BM = 128, BN = 128, THREADS = 128;
-constexpr int KMAX = 256;                   // k of one update (two 128-wide sub-panels)
+constexpr int KMAX = 256;                   // k of one ring stage (longer k: halves)
 constexpr int MAX_SLICES = 8;
 constexpr int NACC = 4;                     // accumulators per pass (4 x 128 TMEM columns)
 constexpr int A_STAGES = 2, B_STAGES = 4;
@@ -114,8 +116,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint8_t* abuf = base;
   uint8_t* bbuf = base + A_STAGES * A_TILE;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = p.slices, kbox = (p.k + 127) / 128;
-  const uint32_t a_bytes = (uint32_t)kbox * BM * 128, b_bytes = (uint32_t)kbox * BN * 128;
+  const int S = p.slices, nkh = (p.k + KMAX - 1) / KMAX;   // k halves of up to KMAX
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < A_STAGES; ++s) { mbar_init(&afull[s], 1); mbar_init(&aempty[s], 1); }
@@ -148,55 +149,64 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int dlo = pass * NACC, dhi = min(S - 1, dlo + NACC - 1);   // diagonals t + u (0-based)
     if (threadIdx.x == 0 && s_fail == 0) {
       bool ok = true;
-      for (int t = 0; t <= dhi && ok; ++t) {
-        const int as = a_issued % A_STAGES;
-        if (a_issued >= A_STAGES && !mbar_wait(&aempty[as], ((a_issued / A_STAGES) & 1) ^ 1)) { ok = false; break; }
-        mbar_expect_tx(&afull[as], a_bytes);
-        for (int kb = 0; kb < kbox; ++kb)
-          tma_load_2d(&ma, &afull[as], abuf + as * A_TILE + kb * BM * 128, kb * 128, t * R + p.a_row0 + row0);
-        ++a_issued;
-        for (int u = max(0, dlo - t); u <= dhi - t; ++u) {
-          const int bs = b_issued % B_STAGES;
-          if (b_issued >= B_STAGES && !mbar_wait(&bempty[bs], ((b_issued / B_STAGES) & 1) ^ 1)) {
-            ok = false;
-            break;
-          }
-          mbar_expect_tx(&bfull[bs], b_bytes);
+      for (int kh = 0; kh < nkh && ok; ++kh) {
+        const int kbox = (min(KMAX, p.k - kh * KMAX) + 127) / 128;
+        const uint32_t a_bytes = (uint32_t)kbox * BM * 128, b_bytes = (uint32_t)kbox * BN * 128;
+        for (int t = 0; t <= dhi && ok; ++t) {
+          const int as = a_issued % A_STAGES;
+          if (a_issued >= A_STAGES && !mbar_wait(&aempty[as], ((a_issued / A_STAGES) & 1) ^ 1)) { ok = false; break; }
+          mbar_expect_tx(&afull[as], a_bytes);
           for (int kb = 0; kb < kbox; ++kb)
-            tma_load_2d(&mb, &bfull[bs], bbuf + bs * B_TILE + kb * BN * 128, kb * 128, u * R + p.b_row0 + col0);
-          ++b_issued;
+            tma_load_2d(&ma, &afull[as], abuf + as * A_TILE + kb * BM * 128, kh * KMAX + kb * 128,
+                        t * R + p.a_row0 + row0);
+          ++a_issued;
+          for (int u = max(0, dlo - t); u <= dhi - t; ++u) {
+            const int bs = b_issued % B_STAGES;
+            if (b_issued >= B_STAGES && !mbar_wait(&bempty[bs], ((b_issued / B_STAGES) & 1) ^ 1)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&bfull[bs], b_bytes);
+            for (int kb = 0; kb < kbox; ++kb)
+              tma_load_2d(&mb, &bfull[bs], bbuf + bs * B_TILE + kb * BN * 128, kh * KMAX + kb * 128,
+                          u * R + p.b_row0 + col0);
+            ++b_issued;
+          }
         }
       }
       if (!ok) s_fail = 1;
     } else if (threadIdx.x == 32 && s_fail == 0) {
       bool ok = true;
-      uint32_t inited = 0;
+      uint32_t inited = 0;   // accumulators written in this pass (the first MMA overwrites)
       fence_after();
-      for (int t = 0; t <= dhi && ok; ++t) {
-        const int as = a_used % A_STAGES;
-        if (!mbar_wait(&afull[as], (a_used / A_STAGES) & 1)) { ok = false; break; }
-        ++a_used;
-        fence_after();
-        const uint32_t a0 = smem_u32(abuf + as * A_TILE);
-        for (int u = max(0, dlo - t); u <= dhi - t; ++u) {
-          const int bs = b_used % B_STAGES;
-          if (!mbar_wait(&bfull[bs], (b_used / B_STAGES) & 1)) { ok = false; break; }
-          ++b_used;
+      for (int kh = 0; kh < nkh && ok; ++kh) {
+        const int kbox = (min(KMAX, p.k - kh * KMAX) + 127) / 128;
+        for (int t = 0; t <= dhi && ok; ++t) {
+          const int as = a_used % A_STAGES;
+          if (!mbar_wait(&afull[as], (a_used / A_STAGES) & 1)) { ok = false; break; }
+          ++a_used;
           fence_after();
-          const uint32_t b0 = smem_u32(bbuf + bs * B_TILE);
-          const int ai = t + u - dlo;
-          const uint32_t acc = tmem + (uint32_t)(ai * BN);
-          for (int kb = 0; kb < kbox; ++kb)
+          const uint32_t a0 = smem_u32(abuf + as * A_TILE);
+          for (int u = max(0, dlo - t); u <= dhi - t; ++u) {
+            const int bs = b_used % B_STAGES;
+            if (!mbar_wait(&bfull[bs], (b_used / B_STAGES) & 1)) { ok = false; break; }
+            ++b_used;
+            fence_after();
+            const uint32_t b0 = smem_u32(bbuf + bs * B_TILE);
+            const int ai = t + u - dlo;
+            const uint32_t acc = tmem + (uint32_t)(ai * BN);
+            for (int kb = 0; kb < kbox; ++kb)
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-              const uint32_t accumulate = ((inited >> ai) & 1u) | (uint32_t)(kb > 0 || kk > 0);
-              mma_i8(acc, smem_desc(a0 + kb * BM * 128 + 32 * kk), smem_desc(b0 + kb * BN * 128 + 32 * kk),
-                     accumulate);
-            }
-          inited |= 1u << ai;
-          mma_commit(&bempty[bs]);
+              for (int kk = 0; kk < 4; ++kk) {
+                const uint32_t accumulate = ((inited >> ai) & 1u) | (uint32_t)(kb > 0 || kk > 0);
+                mma_i8(acc, smem_desc(a0 + kb * BM * 128 + 32 * kk), smem_desc(b0 + kb * BN * 128 + 32 * kk),
+                       accumulate);
+              }
+            inited |= 1u << ai;
+            mma_commit(&bempty[bs]);
+          }
+          mma_commit(&aempty[as]);
         }
-        mma_commit(&aempty[as]);
       }
       s_mma_a = a_used;
       s_mma_b = b_used;

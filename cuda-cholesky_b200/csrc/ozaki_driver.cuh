@@ -3,13 +3,14 @@
 // is ?potrf (lapack/dpotrf.c:172) with the trailing SYRK of every outer block done by
 // the INT8 tensor-core emulation of ozaki.cuh instead of the FP64 DMMA engine.
 //
-// Schedule: the ?potrf schedule (nb = 128, outer blocks of 256 columns as two
-// sub-panels, lookahead depth 1, two streams).  After the two sub-panels of an outer
+// Schedule: the ?potrf schedule (nb = 128, outer blocks of 512 columns as four
+// sub-panels, lookahead depth 1, two streams).  After the sub-panels of an outer
 // block the panel rows below it (the packed buffer P) are cut into S slices
 // (slice_kernel, ping-pong buffers); the lookahead update of the next outer block
 // (panel stream) and the rest of the trailing matrix (update stream) both run on
-// update_kernel from those slices.  The update of the second sub-panel by the first
-// (k = 128) stays on the DMMA engine.
+// update_kernel from those slices, with k = 512: one epilogue per pass over C serves
+// twice the k of a 256-column block.  The updates inside the outer block (each
+// sub-panel's on the ones after it, k = 128) stay on the DMMA engine.
 #include "ozaki.cuh"
 
 namespace {
@@ -50,7 +51,7 @@ CUresult ozaki_update(CULAPACKhandle h, const int8_t* sl, int R, int S, long lon
 }
 
 CUresult potrf_ozaki_run(CULAPACKhandle h, bool upper, int n, double* A, long long lda, int S, long* info) {
-  constexpr int nb = 128, NB = 2 * nb;
+  constexpr int nb = 128, NB = 4 * nb;
   using Smem = DiagSmem<double, nb>;
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
   auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
@@ -93,23 +94,23 @@ CUresult potrf_ozaki_run(CULAPACKhandle h, bool upper, int n, double* A, long lo
           at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
-      if (s0 == 0 && jB > nb) {   // the second sub-panel's columns by the first (DMMA)
+      if (s0 + nb < jB) {   // the outer block's remaining sub-panel columns by this one (DMMA)
         GemmProblem<double> u = problem<double>();
-        u.a = P; u.a_rs = 1; u.a_ks = ldp;
-        u.b = P; u.b_rs = 1; u.b_ks = ldp;
-        u.c = at(j + nb, j + nb); u.c_rs = rs; u.c_cs = cs;
+        u.a = Ps; u.a_rs = 1; u.a_ks = ldp;
+        u.b = Ps; u.b_rs = 1; u.b_ks = ldp;
+        u.c = at(c + nb, c + nb); u.c_rs = rs; u.c_cs = cs;
         u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
         u.alpha = -1.0; u.beta = 1.0;
         u.lower_only = 1;
-        u.m = n - j - nb; u.n = jB - nb; u.k = nb;
+        u.m = n - c - nb; u.n = jB - s0 - nb; u.k = nb;
         CUCHOL_CHECK_CU(gemm<double>(h, u, sp, d_info));
       }
     }
     if (m == 0) break;
-    // slices of the panel rows from j + NB (P rows nb ..), k = jB
+    // slices of the panel rows from j + NB (P rows NB - nb ..), k = jB
     int8_t* sl = sbuf[step & 1];
     int* ex = ebuf[step & 1];
-    oz::slice_kernel<<<(m + 31) / 32, 256, 0, sp>>>(P + nb, 1, ldp, m, jB, S, sl, kp, ex, d_info);
+    oz::slice_kernel<<<(m + 31) / 32, 256, 0, sp>>>(P + (NB - nb), 1, ldp, m, jB, S, sl, kp, ex, d_info);
     ++h->launches;
     CUCHOL_CHECK(cudaGetLastError());
     CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
