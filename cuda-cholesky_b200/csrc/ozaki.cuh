@@ -9,7 +9,8 @@
 //     sum_l P(i, l) P(j, l) ~ 2^(e_i + e_j) sum_{t + u <= S + 1} 2^-7(t + u) (a_t a_u^T)(i, j),
 // and every a_t a_u^T is computed exactly by kind::i8 MMAs with INT32 accumulation; the
 // terms of one diagonal d = t + u share an accumulator (at most S k-long sums of
-// |a| <= 127 products: S * k * 127^2 < 2^31 for k <= 16384 / S).  The epilogue turns
+// |a| <= 127 products: S * k * 127^2 < 2^31 while S * k < 133144; the driver's
+// k <= 2048 with S <= 8 stays eight times below).  The epilogue turns
 // the S accumulators into FP64 (exact), scales them by 2^-7d (exact), sums them in
 // FP64 and applies 2^(e_i + e_j): the only roundings are the final FP64 additions and
 // the dropped terms t + u > S + 1, below 2^-7(S + 1) of |P_i| |P_j| k.

@@ -3,13 +3,15 @@
 // is ?potrf (lapack/dpotrf.c:172) with the trailing SYRK of every outer block done by
 // the INT8 tensor-core emulation of ozaki.cuh instead of the FP64 DMMA engine.
 //
-// Schedule: the ?potrf schedule (nb = 128, outer blocks of 512 columns as four
-// sub-panels, lookahead depth 1, two streams).  After the sub-panels of an outer
+// Schedule: the ?potrf schedule (nb = 128, outer blocks of sub x 128 columns as sub
+// sub-panels, sub from the tuning table: 8 below n = 49152, 16 from there on;
+// lookahead depth 1, two streams).  After the sub-panels of an outer
 // block the panel rows below it (the packed buffer P) are cut into S slices
 // (slice_kernel, ping-pong buffers); the lookahead update of the next outer block
 // (panel stream) and the rest of the trailing matrix (update stream) both run on
-// update_kernel from those slices, with k = 512: one epilogue per pass over C serves
-// twice the k of a 256-column block.  The updates inside the outer block (each
+// update_kernel from those slices, with k = the outer block: the two epilogues per tile
+// (FP64 read-modify-write of C) are paid once per outer block, so a wide block makes
+// the INT8 products dominate.  The updates inside the outer block (each
 // sub-panel's on the ones after it, k = 128) stay on the DMMA engine.
 #include "ozaki.cuh"
 
@@ -51,7 +53,8 @@ CUresult ozaki_update(CULAPACKhandle h, const int8_t* sl, int R, int S, long lon
 }
 
 CUresult potrf_ozaki_run(CULAPACKhandle h, bool upper, int n, double* A, long long lda, int S, long* info) {
-  constexpr int nb = 128, NB = 4 * nb;
+  constexpr int nb = 128;
+  const int NB = (h->potrf_sub > 0 ? h->potrf_sub : tuned_sub(TUNE_OZAKI, 'D', n)) * nb;
   using Smem = DiagSmem<double, nb>;
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
   auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };

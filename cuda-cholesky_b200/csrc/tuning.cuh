@@ -4,13 +4,14 @@
 //
 // Here the tuned values are a versioned, process-wide table of rows
 //   potrf <type S|D|C|Z> <n_min> <sub>
-// meaning: ?potrf of order n >= n_min (the largest such n_min of the type wins) uses
-// outer blocks of sub diagonal blocks (sub x 128 columns; x 64 for Z), i.e. the
-// trailing update's k and the lookahead depth in columns.  The built-in rows below
-// were measured on a B200 (sm_100a, 148 SMs) with cuda-cholesky_b200/cucholesky/tune.py,
-// which writes the same text format; a file in that format replaces the table at run
-// time (cuLAPACKLoadTuning, or the CUCHOLESKY_TUNING environment variable when the
-// first handle is created).  The file's first non-comment line must be
+//   ozaki D <n_min> <sub>
+// meaning: ?potrf (or cuDpotrfOzaki) of order n >= n_min (the largest such n_min of the
+// routine and type wins) uses outer blocks of sub diagonal blocks (sub x 128 columns;
+// x 64 for Z), i.e. the trailing update's k and the lookahead depth in columns.  The
+// built-in rows below were measured on a B200 (sm_100a, 148 SMs); the ?potrf rows are
+// what cuda-cholesky_b200/cucholesky/tune.py writes, in the same text format, and a
+// file in that format replaces the table at run time (cuLAPACKLoadTuning, or the
+// CUCHOLESKY_TUNING environment variable when the first handle is created).  The file's first non-comment line must be
 // "cucholesky-tuning <version>" with the version this library reads (1).
 #pragma once
 
@@ -21,19 +22,27 @@ namespace cuchol {
 constexpr int kTuningVersion = 1;
 constexpr int kMaxSub = 16;
 
+enum TuneKey { TUNE_POTRF = 0, TUNE_OZAKI = 1 };
+
 struct TuneRow {
+  int key;
   char type;
   long long n_min;
   int sub;
 };
 
-// FP64, B200: outer blocks of 2 / 3 / 4 / 6 / 8 diagonal blocks, measured at
-// n = 4096 / 8192 / 16384 / 32768 (best 4.25, 11.22, 56.55, 398.1 ms) and
-// split at the geometric midpoints; the other types keep 2 (not measured).
+// FP64 ?potrf, B200: outer blocks of 2 / 3 / 4 / 6 / 8 diagonal blocks, measured at
+// n = 4096 / 8192 / 16384 / 32768 (best 4.25, 11.22, 56.55, 398.1 ms) and split at the
+// geometric midpoints; the other types keep 2 (not measured).  cuDpotrfOzaki: 8 (1024
+// columns) below n = 49152, 16 from there on (n = 8192 / 32768 / 65536: 10.8 / 255 /
+// 2028 ms with 8; 11.7 / 255 / 1926 ms with 16; 4 gave 282 ms and 2344 ms at the two
+// larger orders).
 inline std::vector<TuneRow>& tuning_rows() {
   static std::vector<TuneRow> rows = {
-      {'D', 0, 2}, {'D', 6144, 3}, {'D', 12288, 4}, {'D', 24576, 6}, {'D', 49152, 8},
-      {'S', 0, 2}, {'C', 0, 2}, {'Z', 0, 2},
+      {TUNE_POTRF, 'D', 0, 2}, {TUNE_POTRF, 'D', 6144, 3}, {TUNE_POTRF, 'D', 12288, 4},
+      {TUNE_POTRF, 'D', 24576, 6}, {TUNE_POTRF, 'D', 49152, 8},
+      {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'C', 0, 2}, {TUNE_POTRF, 'Z', 0, 2},
+      {TUNE_OZAKI, 'D', 0, 8}, {TUNE_OZAKI, 'D', 49152, 16},
   };
   return rows;
 }
@@ -43,19 +52,20 @@ inline std::mutex& tuning_mutex() {
   return m;
 }
 
-// Outer-block size (in diagonal blocks) for ?potrf of order n; 2 when the table has
-// no row for the type.
-inline int tuned_potrf_sub(char type, long long n) {
+// Outer-block size (in diagonal blocks) for the routine `key` of order n; when the
+// table has no row for it, 2 for ?potrf and 8 for the Ozaki factor.
+inline int tuned_sub(int key, char type, long long n) {
   std::lock_guard<std::mutex> lock(tuning_mutex());
-  int sub = 2;
+  int sub = (key == TUNE_OZAKI) ? 8 : 2;
   long long best = -1;
   for (const TuneRow& r : tuning_rows())
-    if (r.type == type && r.n_min <= n && r.n_min > best) {
+    if (r.key == key && r.type == type && r.n_min <= n && r.n_min > best) {
       best = r.n_min;
       sub = r.sub;
     }
   return sub;
 }
+inline int tuned_potrf_sub(char type, long long n) { return tuned_sub(TUNE_POTRF, type, n); }
 
 // Parses a tuning file; false (table unchanged) on any malformed line, unknown
 // version, or a value out of range.
@@ -78,12 +88,14 @@ inline bool load_tuning(const char* path) {
     char key[32], type = 0;
     long long n_min = -1;
     int sub = 0;
-    if (sscanf(p, "%31s %c %lld %d", key, &type, &n_min, &sub) != 4 || strcmp(key, "potrf") != 0 ||
-        strchr("SDCZ", type) == nullptr || n_min < 0 || sub < 1 || sub > kMaxSub) {
+    const bool ozaki = sscanf(p, "%31s", key) == 1 && strcmp(key, "ozaki") == 0;
+    if (sscanf(p, "%31s %c %lld %d", key, &type, &n_min, &sub) != 4 ||
+        (strcmp(key, "potrf") != 0 && !ozaki) || strchr(ozaki ? "D" : "SDCZ", type) == nullptr || n_min < 0 ||
+        sub < 1 || sub > kMaxSub) {
       ok = false;
       break;
     }
-    rows.push_back({type, n_min, sub});
+    rows.push_back({ozaki ? TUNE_OZAKI : TUNE_POTRF, type, n_min, sub});
   }
   fclose(f);
   if (!ok || !have_version) return false;

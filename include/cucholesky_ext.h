@@ -33,9 +33,10 @@ CUresult cuLAPACKGetLaunchCount(CULAPACKhandle, unsigned long long *);
  * cuda-cholesky_b200/cucholesky/tune.py (first line "cucholesky-tuning 1"; the
  * CUCHOLESKY_TUNING environment variable names one to load when the first handle is
  * created).  A malformed file leaves the table unchanged and returns
- * CUDA_ERROR_INVALID_VALUE.  cuLAPACKSetPotrfBlocks overrides the table for one handle
- * (1..16; 0 restores the table); cuLAPACKGetPotrfBlocks reports the value ?potrf of
- * that type and order would use (handle may be NULL: the table alone). */
+ * CUDA_ERROR_INVALID_VALUE.  Rows "ozaki D <n_min> <sub>" do the same for
+ * cuDpotrfOzaki.  cuLAPACKSetPotrfBlocks overrides the table for one handle's ?potrf
+ * and cuDpotrfOzaki (1..16; 0 restores the table); cuLAPACKGetPotrfBlocks reports the
+ * value ?potrf of that type and order would use (handle may be NULL: the table alone). */
 CUresult cuLAPACKLoadTuning(const char *);
 CUresult cuLAPACKSetPotrfBlocks(CULAPACKhandle, int);
 CUresult cuLAPACKGetPotrfBlocks(CULAPACKhandle, char, size_t, int *);

@@ -258,12 +258,14 @@ def test_tuning_table_file(tmp_path):
     bad_version.write_text("cucholesky-tuning 2\npotrf D 0 4\n")
     bad_row = tmp_path / "r.tuning"
     bad_row.write_text("cucholesky-tuning 1\npotrf D 0 99\n")
+    bad_type = tmp_path / "o.tuning"
+    bad_type.write_text("cucholesky-tuning 1\nozaki Z 0 8\n")
     builtin = [(t, n, sub(t, n)) for t in "SDCZ" for n in (100, 7000, 20000, 70000)]
     try:
         assert lib.cuLAPACKLoadTuning(str(good).encode()) == 0
         assert sub("D", 5000) == 2 and sub("D", 6000) == 3 and sub("D", 100000) == 5
         assert sub("S", 10) == 3 and sub("Z", 10) == 2            # no row: 2
-        for f in (bad_version, bad_row, tmp_path / "missing.tuning"):
+        for f in (bad_version, bad_row, bad_type, tmp_path / "missing.tuning"):
             assert lib.cuLAPACKLoadTuning(str(f).encode()) == cucholesky.CUDA_ERROR_INVALID_VALUE
         assert sub("D", 100000) == 5
         assert lib.cuLAPACKGetPotrfBlocks(None, b"Q", 10, C.byref(C.c_int())) == cucholesky.CUDA_ERROR_INVALID_VALUE
@@ -272,7 +274,7 @@ def test_tuning_table_file(tmp_path):
         restore = tmp_path / "builtin.tuning"
         lines = ["cucholesky-tuning 1"]
         lines += ["potrf D 0 2", "potrf D 6144 3", "potrf D 12288 4", "potrf D 24576 6", "potrf D 49152 8",
-                  "potrf S 0 2", "potrf C 0 2", "potrf Z 0 2"]
+                  "potrf S 0 2", "potrf C 0 2", "potrf Z 0 2", "ozaki D 0 8", "ozaki D 49152 16"]
         restore.write_text("\n".join(lines) + "\n")
         assert lib.cuLAPACKLoadTuning(str(restore).encode()) == 0
     assert [(t, n, sub(t, n)) for t in "SDCZ" for n in (100, 7000, 20000, 70000)] == builtin

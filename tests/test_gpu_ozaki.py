@@ -1,7 +1,11 @@
 """cuDpotrfOzaki (FP64 Cholesky with Ozaki-sliced INT8 tensor-core trailing updates)
 through the C ABI: with 8 slices the factor meets the contract's FP64 bound (backward
 error <= 10 in units of n*eps) like cuDpotrf, both storages, ragged n; the info of a
-non-SPD input is the oracle's; fewer slices give a factor of lower accuracy."""
+non-SPD input is the oracle's; fewer slices give a factor of lower accuracy.
+
+The tuned outer block (1024 columns at these orders) would leave a small matrix with no
+trailing update at all, so the tests force 256-column outer blocks on the handle
+(cuLAPACKSetPotrfBlocks), and one test runs every width the table may choose."""
 from __future__ import annotations
 
 import ctypes as C
@@ -16,6 +20,15 @@ from cucholesky import matgen
 pytestmark = pytest.mark.gpu
 
 EPS = np.finfo(np.float64).eps
+
+
+@pytest.fixture(autouse=True)
+def _narrow_outer_blocks(handle):
+    L = cc.lib()
+    L.cuLAPACKSetPotrfBlocks.argtypes = [C.c_void_p, C.c_int]
+    assert L.cuLAPACKSetPotrfBlocks(handle.value, 2) == 0
+    yield
+    assert L.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
 
 
 def _ozaki(handle, uplo, A, slices=8):
@@ -94,3 +107,21 @@ def test_ozaki_seven_slices(handle):
     F7, info = _ozaki(handle, "L", A, 7)
     assert info == 0
     assert _berr(A, F7, "L") <= 10
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_ozaki_outer_block_widths(handle, uplo):
+    """Outer blocks of 256 .. 2048 columns (update launches with k up to 2048, run as
+    256-wide pieces into the same accumulators) all give an FP64-accurate factor, and
+    with 4 slices a visibly less accurate one (the INT8 path did the updates)."""
+    L = cc.lib()
+    n = 4500
+    A = matgen.spd("d", n, seed=21, lda=n + 1)
+    for sub in (2, 4, 8, 16):
+        assert L.cuLAPACKSetPotrfBlocks(handle.value, sub) == 0
+        F, info = _ozaki(handle, uplo, A, 7)
+        assert info == 0
+        assert _berr(A, F, uplo) <= 10, sub
+        F4, info = _ozaki(handle, uplo, A, 4)
+        assert info == 0 and 10 < _berr(A, F4, uplo) < 1e10, sub
+
