@@ -77,10 +77,14 @@ __device__ __forceinline__ bool tri_keep(uint8_t tri, int row, int k) {
 template <typename T> struct SimtCfg { static constexpr int BK = 16; };
 template <> struct SimtCfg<cuDoubleComplex> { static constexpr int BK = 8; };
 
-template <typename T, int LA, int LB>
+// TM x TM outputs per thread (strided by 16), a 16TM x 16TM tile per CTA: TM = 4 for
+// every type in grouped launches; TM = 8 (128 x 128 tiles, 64 FMAs per 16 shared
+// loads) for large single FP32 products with a long k, where the 4 x 4 tile is bound by
+// shared-memory loads.
+template <typename T, int LA, int LB, int TM = 4>
 __global__ void __launch_bounds__(256)
 gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict__ abort_flag) {
-  constexpr int BM = 64, BN = 64, BK = SimtCfg<T>::BK, NT = 256;
+  constexpr int BM = 16 * TM, BN = 16 * TM, BK = SimtCfg<T>::BK, NT = 256;
   constexpr int LDA_PER = BM * BK / NT, LDB_PER = BN * BK / NT;
   if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
 
@@ -98,11 +102,11 @@ gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict_
   const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;
 
-  T acc[4][4];
+  T acc[TM][TM];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = zero<T>();
+    for (int b = 0; b < TM; ++b) acc[a][b] = zero<T>();
 
   T ra[LDA_PER], rb[LDB_PER];
   auto load = [&](int k0) {
@@ -158,15 +162,15 @@ gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict_
       if (more) load(k0 + BK);
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
-        T av[4], bv[4];
+        T av[TM], bv[TM];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) av[a] = As[buf][kk][tx + 16 * a];
+        for (int a = 0; a < TM; ++a) av[a] = As[buf][kk][tx + 16 * a];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = Bs[buf][kk][ty + 16 * b];
+        for (int b = 0; b < TM; ++b) bv[b] = Bs[buf][kk][ty + 16 * b];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < TM; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) mac(acc[a][b], av[a], bv[b]);
+          for (int b = 0; b < TM; ++b) mac(acc[a][b], av[a], bv[b]);
       }
       if (more) {
         store(buf ^ 1);
@@ -177,10 +181,10 @@ gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict_
   }
 
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
+  for (int a = 0; a < TM; ++a) {
     const int i = i0 + tx + 16 * a;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
+    for (int b = 0; b < TM; ++b) {
       const int j = j0 + ty + 16 * b;
       if (i < P.m && j < P.n && (!P.lower_only || i >= j)) {
         T v = mul(P.alpha, acc[a][b]);
