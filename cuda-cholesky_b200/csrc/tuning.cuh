@@ -11,8 +11,9 @@
 // built-in rows below were measured on a B200 (sm_100a, 148 SMs); the ?potrf rows are
 // what cuda-cholesky_b200/cucholesky/tune.py writes, in the same text format, and a
 // file in that format replaces the table at run time (cuLAPACKLoadTuning, or the
-// CUCHOLESKY_TUNING environment variable when the first handle is created).  The file's first non-comment line must be
-// "cucholesky-tuning <version>" with the version this library reads (1).
+// CUCHOLESKY_TUNING environment variable when the first handle is created).  The file's
+// first non-comment line must be "cucholesky-tuning <version>" with the version this
+// library reads (1).
 #pragma once
 
 #include <mutex>
@@ -33,15 +34,19 @@ struct TuneRow {
 
 // FP64 ?potrf, B200: outer blocks of 2 / 3 / 4 / 6 / 8 diagonal blocks, measured at
 // n = 4096 / 8192 / 16384 / 32768 (best 4.25, 11.22, 56.55, 398.1 ms) and split at the
-// geometric midpoints; the other types keep 2 (not measured).  cuDpotrfOzaki: 8 (1024
-// columns) below n = 49152, 16 from there on (n = 8192 / 32768 / 65536: 10.8 / 255 /
-// 2028 ms with 8; 11.7 / 255 / 1926 ms with 16; 4 gave 282 ms and 2344 ms at the two
-// larger orders).
+// geometric midpoints.  S, C, Z: the rows tune.py wrote from n = 4096 / 8192 / 16384
+// (best spotrf 3.93 / 14.27 / 87.34 ms, cpotrf 7.34 / 29.82 / 196.8 ms, zpotrf 11.62 /
+// 61.02 / 436.1 ms; outer block 2 gave 93.65, 208.5 and 507.4 ms at n = 16384).
+// cuDpotrfOzaki: 8 (1024 columns) below n = 49152, 16 from there on (n = 8192 / 32768 /
+// 65536: 10.8 / 255 / 2028 ms with 8; 11.7 / 255 / 1926 ms with 16; 4 gave 282 ms and
+// 2344 ms at the two larger orders).
 inline std::vector<TuneRow>& tuning_rows() {
   static std::vector<TuneRow> rows = {
       {TUNE_POTRF, 'D', 0, 2}, {TUNE_POTRF, 'D', 6144, 3}, {TUNE_POTRF, 'D', 12288, 4},
       {TUNE_POTRF, 'D', 24576, 6}, {TUNE_POTRF, 'D', 49152, 8},
-      {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'C', 0, 2}, {TUNE_POTRF, 'Z', 0, 2},
+      {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'S', 5793, 3}, {TUNE_POTRF, 'S', 11585, 8},
+      {TUNE_POTRF, 'C', 0, 2}, {TUNE_POTRF, 'C', 5793, 3}, {TUNE_POTRF, 'C', 11585, 6},
+      {TUNE_POTRF, 'Z', 0, 3}, {TUNE_POTRF, 'Z', 5793, 6},
       {TUNE_OZAKI, 'D', 0, 8}, {TUNE_OZAKI, 'D', 49152, 16},
   };
   return rows;

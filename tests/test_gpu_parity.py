@@ -265,4 +265,4 @@ def test_outer_block_sizes(handle, p, u):
         assert lib.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
     v = C.c_int(0)
     assert lib.cuLAPACKGetPotrfBlocks(handle.value, p.upper().encode(), 16384, C.byref(v)) == 0
-    assert v.value == (4 if p == "d" else 2)
+    assert v.value == (4 if p == "d" else 6)
