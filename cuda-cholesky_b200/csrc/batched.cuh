@@ -294,23 +294,37 @@ CUresult tune_nb(CUcholBatched p, const BatchedShape<T>& sh, int* best_nb) {
   std::vector<long long> off(sh.batch);
   long long total = 0;
   for (int b = 0; b < sh.batch; ++b) { off[b] = total; total += (long long)sh.n[b] * sh.n[b]; }
-  T* scratch = nullptr;
-  long long* d_off = nullptr;
-  int* d_n = nullptr;
-  CUCHOL_CHECK(cudaMalloc(&scratch, sizeof(T) * std::max<long long>(total, 1)));
-  CUCHOL_CHECK(cudaMalloc(&d_off, sizeof(long long) * sh.batch));
-  CUCHOL_CHECK(cudaMalloc(&d_n, sizeof(int) * sh.batch));
-  CUCHOL_CHECK(cudaMemcpy(d_off, off.data(), sizeof(long long) * sh.batch, cudaMemcpyHostToDevice));
-  CUCHOL_CHECK(cudaMemcpy(d_n, sh.n.data(), sizeof(int) * sh.batch, cudaMemcpyHostToDevice));
+  // everything acquired here is released by `res` on every return path
+  struct Resources {
+    T* scratch = nullptr;
+    long long* d_off = nullptr;
+    int* d_n = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Resources() {
+      if (e0 != nullptr) cudaEventDestroy(e0);
+      if (e1 != nullptr) cudaEventDestroy(e1);
+      cudaFree(scratch);
+      cudaFree(d_off);
+      cudaFree(d_n);
+    }
+  } res;
+  CUCHOL_CHECK(cudaMalloc(&res.scratch, sizeof(T) * std::max<long long>(total, 1)));
+  CUCHOL_CHECK(cudaMalloc(&res.d_off, sizeof(long long) * sh.batch));
+  CUCHOL_CHECK(cudaMalloc(&res.d_n, sizeof(int) * sh.batch));
+  CUCHOL_CHECK(cudaMemcpy(res.d_off, off.data(), sizeof(long long) * sh.batch, cudaMemcpyHostToDevice));
+  CUCHOL_CHECK(cudaMemcpy(res.d_n, sh.n.data(), sizeof(int) * sh.batch, cudaMemcpyHostToDevice));
+  T* scratch = res.scratch;
+  long long* d_off = res.d_off;
+  int* d_n = res.d_n;
   BatchedShape<T> id = sh;
   id.upper = false;
   for (int b = 0; b < sh.batch; ++b) { id.a[b] = scratch + off[b]; id.lda[b] = sh.n[b]; }
   float best = 1e30f;
   *best_nb = kBatchedMaxNb;
   cudaStream_t s = p->h->s_update;
-  cudaEvent_t e0, e1;
-  CUCHOL_CHECK(cudaEventCreate(&e0));
-  CUCHOL_CHECK(cudaEventCreate(&e1));
+  CUCHOL_CHECK(cudaEventCreate(&res.e0));
+  CUCHOL_CHECK(cudaEventCreate(&res.e1));
+  cudaEvent_t e0 = res.e0, e1 = res.e1;
   CUresult rc = CUDA_SUCCESS;
   for (int nb : candidates) {
     rc = build_graph<T>(p, id, nb);
@@ -329,12 +343,7 @@ CUresult tune_nb(CUcholBatched p, const BatchedShape<T>& sh, int* best_nb) {
     if (rc != CUDA_SUCCESS) break;
     if (ms_min < best) { best = ms_min; *best_nb = nb; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   free_plan_memory(p);
-  cudaFree(scratch);
-  cudaFree(d_off);
-  cudaFree(d_n);
   return rc;
 }
 

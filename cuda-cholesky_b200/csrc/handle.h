@@ -29,6 +29,7 @@ struct __culapackhandle_st {
   unsigned long long launches;   // kernels launched by this handle
   int force_simt;                // testing: route FP64 products to the SIMT engine
   int potrf_sub;                 // ?potrf outer block in diagonal blocks (0: tuning table)
+  int lauum_cols;                // testing: ?lauum block-column width (0: from the workspace cap)
 };
 
 namespace cuchol {

@@ -545,25 +545,44 @@ CUresult trtri_run(CULAPACKhandle h, bool upper, bool unit, int n, T* A, long lo
 }
 
 // ---- ?LAUUM ---------------------------------------------------------------------
-// L^H L (lower; U U^H upper via the transposed view): every lower tile of the
-// result C(i, j) = sum_{k >= max(i,j)} conj(L(k, i)) L(k, j) is independent, so the
-// product is one launch into workspace, followed by a copy of its lower triangle
-// back into A.
+// L^H L (lower; U U^H upper via the transposed view), in place.  The lower part of
+// the result, C(i, j) = sum_{k >= i} conj(L(k, i)) L(k, j) for i >= j, reads only
+// columns >= j of L.  So the block columns of C are formed left to right, each as one
+// product into workspace and then copied over the same block column of A: the
+// columns a later block reads are still untouched when it runs.  The block width w
+// keeps the workspace ((n - j0) x w) within kLauumWorkspace bytes; orders whose
+// whole product fits take one launch.
+constexpr size_t kLauumWorkspace = size_t(512) << 20;
+
+template <typename T>
+int lauum_width(CULAPACKhandle h, int n) {
+  if (h->lauum_cols > 0) return std::min(h->lauum_cols, n);
+  const size_t cols = kLauumWorkspace / (sizeof(T) * round_up((size_t)n, 2));
+  if (cols >= (size_t)n) return n;
+  return (int)std::max<size_t>(256, cols / 256 * 256);
+}
+
 template <typename T>
 CUresult lauum_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda) {
   const long long rs = upper ? lda : 1, cs = upper ? 1 : lda;
+  auto at = [&](long long i, long long j) { return A + i * rs + j * cs; };
   cudaStream_t sp = h->s_panel;
+  const int w = lauum_width<T>(h, n);
   const long long ldw = (long long)round_up((size_t)n, 2);
-  CUCHOL_CHECK_CU(ensure_workspace(h, sizeof(T) * (size_t)ldw * n));
+  CUCHOL_CHECK_CU(ensure_workspace(h, sizeof(T) * (size_t)ldw * w));
   T* W = static_cast<T*>(h->ws);
-  GemmProblem<T> p = problem<T>();
-  p.a = A; p.a_rs = cs; p.a_ks = rs; p.conj_a = 1; p.tri_a = TRI_UPPER;
-  p.b = A; p.b_rs = cs; p.b_ks = rs; p.tri_b = TRI_UPPER;
-  p.c = W; p.c_rs = 1; p.c_cs = ldw;
-  p.m = n; p.n = n; p.k = n;
-  p.lower_only = 1; p.real_diag = 1;
-  CUCHOL_CHECK_CU(gemm<T>(h, p, sp, nullptr));
-  CUCHOL_CHECK_CU(copy_view<T>(h, W, 1, ldw, A, rs, cs, n, n, true, sp, nullptr));
+  for (int j0 = 0; j0 < n; j0 += w) {
+    const int cols = std::min(w, n - j0), m = n - j0;
+    // C(i', j') = sum_k' conj(L(j0 + k', j0 + i')) L(j0 + k', j0 + j'),  k' >= i' >= j'
+    GemmProblem<T> p = problem<T>();
+    p.a = at(j0, j0); p.a_rs = cs; p.a_ks = rs; p.conj_a = 1; p.tri_a = TRI_UPPER;
+    p.b = at(j0, j0); p.b_rs = cs; p.b_ks = rs; p.tri_b = TRI_UPPER;
+    p.c = W; p.c_rs = 1; p.c_cs = ldw;
+    p.m = m; p.n = cols; p.k = m;
+    p.lower_only = 1; p.real_diag = 1;
+    CUCHOL_CHECK_CU(gemm<T>(h, p, sp, nullptr));
+    CUCHOL_CHECK_CU(copy_view<T>(h, W, 1, ldw, at(j0, j0), rs, cs, m, cols, true, sp, nullptr));
+  }
   CUCHOL_CHECK(cudaStreamSynchronize(sp));
   return CUDA_SUCCESS;
 }
@@ -634,6 +653,8 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   {
     const char* e = getenv("CUCHOLESKY_FORCE_SIMT");   // testing: FP64 products on the SIMT engine
     h->force_simt = (e != nullptr && e[0] == '1') ? 1 : 0;
+    const char* c = getenv("CUCHOLESKY_LAUUM_COLS");   // testing: ?lauum block-column width
+    h->lauum_cols = (c != nullptr) ? std::max(0, atoi(c)) : 0;
   }
   {
     // a tuning file named by the environment replaces the built-in table once

@@ -67,18 +67,43 @@ logdet_static_kernel(const double* __restrict__ x, long long incx, long long n, 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 Scratch* g_addr[kMaxDevices] = {};
+CUcontext g_ctx[kMaxDevices] = {};   // the context each cached address belongs to
 
-// Device address of g_scratch on the current device, looked up on the first call
-// for that device (with that device current) and cached.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// The driver's cuCtxGetCurrent (this library links only the CUDA runtime).
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// Device address of g_scratch on the current device, looked up (with that device
+// current) on the first call for the device and cached together with the device's
+// context: a context created since (after cudaDeviceReset the module is loaded
+// again and the array may sit elsewhere) triggers a fresh lookup.
 CUresult scratch_address(Scratch** out) {
   int dev = 0;
   CUCHOL_CHECK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return CUDA_ERROR_INVALID_DEVICE;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (get == nullptr) return CUDA_ERROR_NOT_FOUND;
+  CUcontext ctx = nullptr;   // null before the runtime has made a context current
+  CUresult rc = get(&ctx);
+  if (rc != CUDA_SUCCESS) return rc;
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (g_addr[dev] == nullptr) {
+  if (ctx == nullptr || g_addr[dev] == nullptr || g_ctx[dev] != ctx) {
     void* p = nullptr;
-    CUCHOL_CHECK(cudaGetSymbolAddress(&p, g_scratch));
+    CUCHOL_CHECK(cudaGetSymbolAddress(&p, g_scratch));   // makes the device's context current
+    if ((rc = get(&ctx)) != CUDA_SUCCESS) return rc;
     g_addr[dev] = static_cast<Scratch*>(p);
+    g_ctx[dev] = ctx;
   }
   *out = g_addr[dev];
   return CUDA_SUCCESS;

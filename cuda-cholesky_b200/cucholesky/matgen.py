@@ -119,3 +119,108 @@ def scaled_spd_device(n: int, k: float, seed: int = 0, device: str = "cuda"):
     A *= d[None, :]
     del G
     return A
+
+
+# ---------------------------------------------------------------------------------
+# Device-side inputs and error estimates for large orders (torch, FP64 arithmetic).
+# A device matrix is a torch tensor T of shape (n, n) holding the column-major
+# matrix M, i.e. M = T.T (T[j, i] = M(i, j)); for a Hermitian input T = conj(M).
+# ---------------------------------------------------------------------------------
+_TORCH_DT = {"s": "float32", "d": "float64", "c": "complex64", "z": "complex128"}
+_EPS = {"s": 2.0 ** -23, "d": 2.0 ** -52, "c": 2.0 ** -23, "z": 2.0 ** -52}
+
+
+def spd_device(p: str, n: int, seed: int = 0, device: str = "cuda"):
+    """The ``spd`` family on the device (torch Philox, FP64 product), returned as
+    the FP64 / complex128 tensor T of the column-major matrix (see above); round it
+    to the routine's type with ``T.to(torch_dtype(p))``."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    if p in "sd":
+        G = torch.rand((n, n), generator=g, device=device, dtype=torch.float64) * 2 - 1
+        A = G @ G.T
+    else:
+        G = torch.randn((n, n), generator=g, device=device, dtype=torch.complex128)   # Re, Im ~ N(0, 1/2)
+        A = G @ G.conj().T
+    del G
+    A /= n
+    A.diagonal().add_(1.0)
+    if p in "cz":
+        A.diagonal().imag.zero_()
+    return A.T.contiguous() if p in "cz" else A     # T = M^T (= conj(M) for Hermitian M)
+
+
+def torch_dtype(p: str):
+    import torch
+    return getattr(torch, _TORCH_DT[p])
+
+
+def _wide(T):
+    import torch
+    return T.to(torch.complex128 if T.is_complex() else torch.float64)
+
+
+def factor_of(T, uplo: str):
+    """L with A = L L^H from the factor a cu?potrf call left in T (FP64 copy)."""
+    import torch
+    M = _wide(T).T
+    if uplo == "L":
+        return torch.tril(M)
+    return torch.triu(M).conj().T.contiguous()
+
+
+def hermitian_of(T, uplo: str):
+    """The full Hermitian matrix whose `uplo` triangle T holds (FP64 copy)."""
+    import torch
+    M = _wide(T).T
+    H = torch.tril(M) if uplo == "L" else torch.triu(M)
+    off = torch.tril(H, -1) if uplo == "L" else torch.triu(H, 1)
+    H = H + off.conj().T
+    if H.is_complex():
+        H.diagonal().imag.zero_()
+    return H
+
+
+def _probes(n, k, like, seed):
+    import torch
+    g = torch.Generator(device=like.device)
+    g.manual_seed(seed)
+    return torch.randn((n, k), generator=g, device=like.device, dtype=like.dtype)
+
+
+def probe_backward_error(A, L, p: str, k: int = 8, seed: int = 1234) -> float:
+    """||A - L L^H||_F / (n eps ||A||_F) estimated with k Gaussian probes X:
+    E[||E X||_F^2] = k ||E||_F^2.  A: full FP64 matrix, L: FP64 factor."""
+    import torch
+    n = A.shape[0]
+    X = _probes(n, k, A, seed)
+    R = A @ X - L @ (L.conj().T @ X)
+    return float(torch.linalg.norm(R).item() / k ** 0.5 / (n * _EPS[p] * torch.linalg.norm(A).item()))
+
+
+def cond2(A, Ainv, iters: int = 60, seed: int = 99) -> float:
+    """2-norm condition number of Hermitian positive definite A from power
+    iterations on A and on its computed inverse (a slight underestimate)."""
+    import torch
+
+    def lmax(M):
+        v = _probes(M.shape[0], 1, M, seed)
+        lam = 0.0
+        for _ in range(iters):
+            w = M @ v
+            lam = torch.linalg.norm(w).item()
+            v = w / lam
+        return lam
+    return lmax(A) * lmax(Ainv)
+
+
+def probe_inverse_residual(A, Ainv, p: str, kappa: float | None = None, k: int = 8, seed: int = 4321) -> float:
+    """||I - A Ainv||_F / (n kappa eps) estimated with k Gaussian probes."""
+    import torch
+    n = A.shape[0]
+    if kappa is None:
+        kappa = cond2(A, Ainv)
+    X = _probes(n, k, A, seed)
+    R = X - A @ (Ainv @ X)
+    return float(torch.linalg.norm(R).item() / k ** 0.5 / (n * kappa * _EPS[p]))

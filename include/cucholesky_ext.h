@@ -86,9 +86,13 @@ CUresult cuCholBatchedDestroy(CUcholBatched);
  * larger n calls XERBLA with position 3 and returns CUDA_ERROR_INVALID_VALUE.
  * The work is queued on `stream`; *result is valid once the stream has
  * synchronised.  The first call on each device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current, so make that first
- * call before any stream capture.  All calls share the one array and each call
- * clears what must start at zero: calls that overlap on the GPU race. */
+ * address (cudaGetSymbolAddress) with that device current, and so does the first
+ * call after the device's context was re-created (cudaDeviceReset): make that
+ * first call before any stream capture.  Under lazy module loading (CUDA's
+ * default) that first call can also make the driver load this library's kernels,
+ * which takes device memory once; make it at start-up, or set
+ * CUDA_MODULE_LOADING=EAGER.  All calls share the one array and each call clears
+ * what must start at zero: calls that overlap on the GPU race. */
 CUresult cuDlogdetNoAlloc(CUdeviceptr x, size_t incx, size_t n, double *result, CUstream stream);
 
 

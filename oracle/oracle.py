@@ -36,7 +36,7 @@ def _lib(impl: str) -> C.CDLL:
     if impl not in _libs:
         path = PORT_LIB if impl == "port" else REF_LIB
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} is not built (make -f oracle/Makefile [ref])")
+            raise FileNotFoundError(f"{path} is not built (make -f oracle/Makefile [ref REF=<reference tree>])")
         lib = C.CDLL(path)
         if impl == "reference":
             # the reference prints a message through its XERBLA hook on argument

@@ -2,7 +2,8 @@
 # its sources where they lie, into oracle/_ref/libref.so.  Test infrastructure only:
 # the library is the checker and the CPU baseline, never part of the product.
 #
-#   make -f oracle/ref.mk            (REF defaults to the mounted reference tree)
+#   make -f oracle/ref.mk REF=<reference tree>
+#   (or CUCHOLESKY_REFERENCE=<reference tree> make -f oracle/ref.mk)
 #
 # The reference sources are not copied into this repository.  Three generated shims
 # (written under oracle/_ref/shim/ only) let them compile on the CPU without a GPU:
@@ -17,7 +18,10 @@
 #
 # No -ffast-math (reference lapack/Makefile:9 uses it): isnan() must survive so the
 # info return on NaN inputs matches the source semantics.
-REF   ?= /root/reference
+REF   ?= $(CUCHOLESKY_REFERENCE)
+ifeq ($(strip $(REF)),)
+$(error set REF or CUCHOLESKY_REFERENCE to the reference source tree)
+endif
 HERE  := $(dir $(lastword $(MAKEFILE_LIST)))
 OUT   := $(HERE)_ref
 SHIM  := $(OUT)/shim

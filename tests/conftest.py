@@ -13,7 +13,9 @@ for sub in ("oracle", "cuda-cholesky_b200"):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE_TREE = "/root/reference"
+# The reference's source tree, when a test run should (re)build its CPU library
+# into oracle/_ref (normally __graft_entry__.build() has built it already).
+REFERENCE_TREE = os.environ.get("CUCHOLESKY_REFERENCE", "")
 
 
 def pytest_configure(config):
@@ -23,8 +25,9 @@ def pytest_configure(config):
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile")], check=True)
     if (not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref.so"))
-            and os.path.isdir(REFERENCE_TREE)):
-        subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "ref"], check=False)
+            and REFERENCE_TREE and os.path.isdir(REFERENCE_TREE)):
+        subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "ref",
+                        f"REF={REFERENCE_TREE}"], check=False)
 
 
 @pytest.fixture(scope="session")

@@ -40,7 +40,7 @@ def cases():
 
 def main() -> None:
     if not O.available("reference"):
-        raise SystemExit("oracle/_ref/libref.so is not built (make -f oracle/Makefile ref)")
+        raise SystemExit("oracle/_ref/libref.so is not built (make -f oracle/Makefile ref REF=<reference tree>)")
     out = {}
     for p, u, n, lda, bad in cases():
         A = matgen.spd(p, n, seed=1000 + n, lda=lda)

@@ -239,22 +239,24 @@ def test_determinism(handle):
     assert np.array_equal(X1, X2)
 
 
-@pytest.mark.parametrize("p", list("dz"))
+@pytest.mark.parametrize("p", list("sdcz"))
 @pytest.mark.parametrize("u", ["L", "U"])
 def test_outer_block_sizes(handle, p, u):
-    """Every ?potrf outer-block size the tuning table may choose (1..8 diagonal
+    """Every ?potrf outer-block size the tuning table accepts (1..16 diagonal
     blocks, here forced per handle) gives a factor within the bounds, on an order
-    that leaves a partial outer block; the table's own choice is restored after."""
+    that leaves a partial outer block and, at the widest blocks, trailing updates
+    with k >= 1024 over >= 256 rows (the large-tile FP32 path); the table's own
+    choice is restored after."""
     import ctypes as C
     from cucholesky import tune
     lib = cc.lib()
     tune._declare(lib)
-    n, lda = 1100, 1103
+    n, lda = 2200, 2203
     A = matgen.spd(p, n, seed=5, lda=lda)
     Fo = A.copy(order="F")
     assert O.potrf(p, u, Fo, lda=lda) == 0
     try:
-        for sub in (1, 2, 3, 4, 6, 8):
+        for sub in (1, 2, 3, 4, 5, 6, 8, 12, 16):
             assert lib.cuLAPACKSetPotrfBlocks(handle.value, sub) == 0
             F, info = gpu_call(handle, "potrf", p, u, A)
             assert info == 0
@@ -264,5 +266,39 @@ def test_outer_block_sizes(handle, p, u):
     finally:
         assert lib.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
     v = C.c_int(0)
+    tune_expected = {"d": 4, "z": 6, "s": 8, "c": 6}
     assert lib.cuLAPACKGetPotrfBlocks(handle.value, p.upper().encode(), 16384, C.byref(v)) == 0
-    assert v.value == (4 if p == "d" else 6)
+    assert v.value == tune_expected[p]
+
+
+@pytest.mark.parametrize("p", list("sdcz"))
+def test_lauum_in_place_block_columns(p):
+    """?lauum forms the product one block column at a time in place; a handle whose
+    block width is forced small (CUCHOLESKY_LAUUM_COLS, read at handle creation)
+    runs several block columns, including a ragged last one."""
+    import os
+    old = os.environ.get("CUCHOLESKY_LAUUM_COLS")
+    os.environ["CUCHOLESKY_LAUUM_COLS"] = "256"
+    try:
+        h = cc.Handle()
+    finally:
+        if old is None:
+            del os.environ["CUCHOLESKY_LAUUM_COLS"]
+        else:
+            os.environ["CUCHOLESKY_LAUUM_COLS"] = old
+    try:
+        for u in "LU":
+            n, lda = 700, 703
+            A = matgen.spd(p, n, seed=23, lda=lda)
+            Fo = A.copy(order="F")
+            assert O.potrf(p, u, Fo, lda=lda) == 0
+            Lm, _ = gpu_call(h, "lauum", p, u, Fo)
+            Lo = Fo.copy(order="F")
+            O.lauum(p, u, Lo)          # the oracle takes lda from the array's rows
+            d = np.abs(_tri(u)(Lm[:n, :n] - Lo[:n, :n])).max() / np.abs(Lo[:n, :n]).max()
+            assert d <= 100 * n * EPS[p], (u, d)
+            other = np.triu(np.ones((n, n), bool), 1) if u == "L" else np.tril(np.ones((n, n), bool), -1)
+            assert np.array_equal(Lm[:n, :n][other], Fo[:n, :n][other])
+            assert np.array_equal(Lm[n:, :], Fo[n:, :])
+    finally:
+        h.close()

@@ -67,6 +67,23 @@ def test_noalloc_matches_cudlogdet_twice(handle):
         assert abs(second - ref) <= tol, (m, second, ref)
 
 
+def test_noalloc_allocates_nothing_after_first_call():
+    """After a first call on the device (which may load the library's kernels), a
+    call leaves the device's free memory exactly unchanged: it allocates nothing."""
+    import torch
+    x = torch.from_numpy(np.random.default_rng(5).uniform(0.5, 2.0, 300_000)).cuda()
+    _noalloc_logdet(x.data_ptr(), 1, x.numel())            # warm-up: module load, address lookup
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    out = C.c_double(float("nan"))
+    for _ in range(3):
+        assert _noalloc()(x.data_ptr(), 1, x.numel(), C.byref(out), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert np.isfinite(out.value)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     out = C.c_double(1.0)
     assert _noalloc()(0, 1, MAX_N + 1, C.byref(out), None) == cc.CUDA_ERROR_INVALID_VALUE
