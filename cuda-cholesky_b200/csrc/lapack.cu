@@ -16,6 +16,7 @@
 #include "diag.cuh"
 #include "dmma.cuh"
 #include "gemm.cuh"
+#include "zmma.cuh"
 #include "handle.h"
 #include "panel.cuh"
 #include "trsm.cuh"
@@ -214,12 +215,100 @@ bool try_dmma(CULAPACKhandle h, const GemmProblem<double>& p, cudaStream_t s, co
   return true;
 }
 
+// ---- complex FP64 tensor-core path (zmma.cuh) -------------------------------------
+// A complex view as an FP64 TMA map (128-byte swizzle): layout R (rows contiguous)
+// is the real matrix of 2 * rows x k doubles, boxes of 16 doubles (8 complex rows)
+// x 8 k; layout K (k contiguous) is rows x 2k doubles, boxes of 16 doubles (8
+// complex k) x box_rows rows.  Any leading dimension works: its byte stride is a
+// multiple of 16.
+bool make_zmap(CUtensorMap* map, const cuDoubleComplex* base, int layout, long long rows, long long k,
+               long long ld, int box_rows) {
+  EncodeTiledFn fn = encode_tiled();
+  if (fn == nullptr) return false;
+  cuuint64_t dims[2], strides[1] = {(cuuint64_t)ld * sizeof(cuDoubleComplex)};
+  cuuint32_t box[2], estr[2] = {1, 1};
+  if (layout == dmma::LAYOUT_R) {
+    dims[0] = 2 * rows; dims[1] = k; box[0] = 16; box[1] = zmma::BK;
+  } else {
+    dims[0] = 2 * k; dims[1] = rows; box[0] = 16; box[1] = box_rows;
+  }
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<cuDoubleComplex*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int LA, int LB, bool TRI>
+CUresult launch_zmma(CULAPACKhandle h, const CUtensorMap& ma, const CUtensorMap& mb, const zmma::Params& q,
+                     int tiles, cudaStream_t s, const int* abort) {
+  static bool attr = false;
+  if (!attr) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      zmma::SMEM_BYTES));
+    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    attr = true;
+  }
+  zmma::gemm_kernel<LA, LB, TRI><<<tiles, zmma::THREADS, zmma::SMEM_BYTES, s>>>(ma, mb, q, abort);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
+template <bool TRI>
+CUresult launch_zmma_layouts(CULAPACKhandle h, int la, int lb, const CUtensorMap& ma, const CUtensorMap& mb,
+                             const zmma::Params& q, int tiles, cudaStream_t s, const int* abort) {
+  if (la == 0 && lb == 0) return launch_zmma<0, 0, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 1) return launch_zmma<0, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 1 && lb == 0) return launch_zmma<1, 0, TRI>(h, ma, mb, q, tiles, s, abort);
+  return launch_zmma<1, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+}
+
+// Runs a complex double problem on the FP64 tensor-core engine when both operand
+// views are row- or k-contiguous and 16-byte aligned; false (nothing launched)
+// otherwise.
+bool try_zmma(CULAPACKhandle h, const GemmProblem<cuDoubleComplex>& p, cudaStream_t s, const int* abort,
+              CUresult* rc) {
+  const int la = (p.a_rs == 1) ? dmma::LAYOUT_R : (p.a_ks == 1 ? dmma::LAYOUT_K : -1);
+  const int lb = (p.b_rs == 1) ? dmma::LAYOUT_R : (p.b_ks == 1 ? dmma::LAYOUT_K : -1);
+  if (la < 0 || lb < 0 || p.k <= 0) return false;
+  const long long lda = (la == dmma::LAYOUT_R) ? p.a_ks : p.a_rs;
+  const long long ldb = (lb == dmma::LAYOUT_R) ? p.b_ks : p.b_rs;
+  if (!aligned16(p.a) || !aligned16(p.b)) return false;
+  CUtensorMap ma, mb;
+  if (!make_zmap(&ma, p.a, la, p.m, p.k, lda, zmma::BM) || !make_zmap(&mb, p.b, lb, p.n, p.k, ldb, zmma::BN))
+    return false;
+  zmma::Params q;
+  q.c = p.c; q.c_rs = p.c_rs; q.c_cs = p.c_cs;
+  q.cin = p.cin; q.cin_rs = p.cin_rs; q.cin_cs = p.cin_cs;
+  q.m = p.m; q.n = p.n; q.k = p.k;
+  q.alpha = p.alpha; q.beta = p.beta;
+  q.conj_a = p.conj_a; q.conj_b = p.conj_b;
+  q.tri_a = p.tri_a; q.tri_b = p.tri_b; q.unit_a = p.unit_a; q.unit_b = p.unit_b;
+  q.lower_only = p.lower_only; q.real_diag = p.real_diag;
+  q.tiles_m = (p.m + zmma::BM - 1) / zmma::BM;
+  q.tiles_n = (p.n + zmma::BN - 1) / zmma::BN;
+  const bool unit_alpha = p.alpha.y == 0.0 && (p.alpha.x == 1.0 || p.alpha.x == -1.0);
+  q.preload = unit_alpha &&
+              (p.cin == nullptr || (p.cin_rs == p.c_rs && p.cin_cs == p.c_cs) || p.cin != p.c);
+  q.neg = q.preload && p.alpha.x == -1.0;
+  q.err = h->d_words + 3;
+  const int tiles = q.tiles_m * q.tiles_n;
+  const bool tri = p.tri_a || p.tri_b || p.unit_a || p.unit_b;
+  *rc = tri ? launch_zmma_layouts<true>(h, la, lb, ma, mb, q, tiles, s, abort)
+            : launch_zmma_layouts<false>(h, la, lb, ma, mb, q, tiles, s, abort);
+  return true;
+}
+
 template <typename T>
 CUresult gemm(CULAPACKhandle h, GemmProblem<T> p, cudaStream_t s, const int* abort) {
   if (p.m <= 0 || p.n <= 0) return CUDA_SUCCESS;
   if constexpr (std::is_same<T, double>::value) {
     CUresult rc;
     if (!h->force_simt && try_dmma(h, p, s, abort, &rc)) return rc;
+  }
+  if constexpr (std::is_same<T, cuDoubleComplex>::value) {
+    CUresult rc;
+    if (!h->force_simt && try_zmma(h, p, s, abort, &rc)) return rc;
   }
   GemmLaunch<T> L{};
   L.list = nullptr;
