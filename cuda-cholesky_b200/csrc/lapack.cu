@@ -399,13 +399,12 @@ CUresult set_smem(const void* fn, size_t bytes) {
 // Right-looking blocked Cholesky, outer blocks of NB = sub*nb columns (each factored
 // as sub nb-wide sub-panels; sub from the tuning table, 2 to 8 by n for FP64),
 // lookahead depth 1, on two streams:
-//   panel stream : for each sub-panel: diagonal-block factor (+ inverse W for complex
-//                  types) -> panel solve into the packed buffer P -> the update of the
-//                  outer block's remaining sub-panel columns by it.  Then [wait
-//                  previous trailing update] -> update of the next outer block
-//                  (lookahead, k = NB)
-//   update stream: [wait panel] -> (complex: copy P into A) -> update of the rest of
-//                  the trailing matrix (k = NB)
+//   panel stream : for each sub-panel: diagonal-block factor -> row-parallel panel
+//                  solve (into A and the packed buffer P) -> the update of the outer
+//                  block's remaining sub-panel columns by it.  Then [wait previous
+//                  trailing update] -> update of the next outer block (lookahead,
+//                  k = NB)
+//   update stream: [wait panel] -> update of the rest of the trailing matrix (k = NB)
 // The next outer block is factored on a few SMs while the trailing update of the
 // previous one runs on the rest; a wider outer block cuts the trailing update's
 // tiles per flop (their fill and drain are the engine's overhead) at the price of
@@ -438,17 +437,14 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   int* d_info = h->d_words;
 
   const long long ldp = (long long)round_up((size_t)n, 2);
-  const size_t ws = sizeof(T) * ((size_t)nb * nb + 2 * (size_t)ldp * NB);
+  const size_t ws = sizeof(T) * (2 * (size_t)ldp * NB);
   CUCHOL_CHECK_CU(ensure_workspace(h, ws));
-  T* winv = static_cast<T*>(h->ws);
-  T* pbuf[2] = {winv + (size_t)nb * nb, winv + (size_t)nb * nb + (size_t)ldp * NB};
+  T* pbuf[2] = {static_cast<T*>(h->ws), static_cast<T*>(h->ws) + (size_t)ldp * NB};
 
   CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_factor_kernel<T, nb, kDiagThreads2>, Smem::bytes));
-  // real types: the panel solve is a row-parallel triangular solve (no inverse of the
-  // diagonal block); complex types: inverse W, then P = A21 W^H on the GEMM engine
-  constexpr bool kReal = std::is_same<T, double>::value || std::is_same<T, float>::value;
-  if constexpr (kReal)
-    CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, false>, trsm_rows_smem<T>()));
+  // the panel solve is a row-parallel triangular solve (no inverse of the diagonal
+  // block) that writes the solved rows into A and into P
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, false>, trsm_rows_smem<T>()));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
   CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
   // the update stream starts after the panel stream's initialisation
@@ -480,7 +476,7 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
       const int c = j + s0, jb = std::min(nb, j + jB - c);
       const int mr = n - c - jb;                 // rows below this diagonal block
       diag_factor_kernel<T, nb, kDiagThreads2><<<1, kDiagThreads2, Smem::bytes, sp>>>(
-          at(c, c), rs, cs, jb, (mr > 0 && !kReal) ? winv : nullptr, nb, c, d_info, h->d_logdet);
+          at(c, c), rs, cs, jb, nullptr, nb, c, d_info, h->d_logdet);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (mr == 0) {
@@ -489,27 +485,13 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
       }
       // panel solve into P: rows c + jb .. n-1 are P rows s0 .. (P starts at j + nb)
       T* Ps = P + s0 + (long long)s0 * ldp;
-      if constexpr (kReal) {
-        // row-parallel triangular solve: A21 := A21 L11^-T in place, and into P
-        trsm_rows_kernel<T, T, T, T, false><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
-            at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
-        ++h->launches;
-        CUCHOL_CHECK(cudaGetLastError());
-        CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
-        if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, sp));
-      } else {
-        GemmProblem<T> t = problem<T>();
-        t.a = at(c + jb, c); t.a_rs = rs; t.a_ks = cs;
-        t.b = winv; t.b_rs = 1; t.b_ks = nb; t.conj_b = 1;   // zeros above W's diagonal
-        t.c = Ps; t.c_rs = 1; t.c_cs = ldp;
-        t.m = mr; t.n = jb; t.k = jb;
-        CUCHOL_CHECK_CU(gemm<T>(h, t, sp, d_info));
-        CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
-        // update stream: the solved rows into A, off the panel stream's critical path
-        CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
-        CUCHOL_CHECK_CU(copy_view<T>(h, Ps, 1, ldp, at(c + jb, c), rs, cs, mr, jb, false, su, d_info));
-        if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, su));
-      }
+      // row-parallel triangular solve: A21 := A21 L11^-H in place, and into P
+      trsm_rows_kernel<T, T, T, T, false><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
+          at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
+      ++h->launches;
+      CUCHOL_CHECK(cudaGetLastError());
+      CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
+      if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, sp));
       if (s0 + nb < jB) {
         // the outer block's remaining sub-panel columns (rows c + nb ..) by this one
         const T* Pc = P + s0 + (long long)s0 * ldp;

@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include "scalar.cuh"
 
 namespace cuchol {
 
@@ -19,21 +20,42 @@ template <typename Op> __device__ __forceinline__ Op to_op(float x);
 template <> __device__ __forceinline__ __nv_bfloat16 to_op<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
 template <> __device__ __forceinline__ float to_op<float>(float x) { return round_tf32(x); }
 
-// Panel solve X = B L^-T in place, row-parallel: B (m x jb, jb <= 128, logical view
-// B(i, j) = B[i*brs + j*bcs]) is overwritten by X, and X also goes to out2
-// (out2[i*o_rs + j*o_cs]; ROUND: rounded to the tensor-core operand type O2, BF16
-// or TF32, else a plain conversion).  L: the factored jb x jb diagonal block
-// (view strides lrs, lcs).  CTA: 64 rows; thread (r, cg) holds columns
+// Conversions between the element types the panel solve reads and writes (the
+// complex types are only ever converted to themselves).
+template <typename D, typename S> __device__ __forceinline__ D cvt(S x) {
+  if constexpr (Traits<D>::complex) return x;
+  else return (D)x;
+}
+// acc -= a * b
+__device__ __forceinline__ void msub(float& acc, float a, float b) { acc = fmaf(-a, b, acc); }
+__device__ __forceinline__ void msub(double& acc, double a, double b) { acc = fma(-a, b, acc); }
+__device__ __forceinline__ void msub(cuFloatComplex& acc, cuFloatComplex a, cuFloatComplex b) {
+  acc.x = fmaf(-a.x, b.x, acc.x); acc.x = fmaf(a.y, b.y, acc.x);
+  acc.y = fmaf(-a.x, b.y, acc.y); acc.y = fmaf(-a.y, b.x, acc.y);
+}
+__device__ __forceinline__ void msub(cuDoubleComplex& acc, cuDoubleComplex a, cuDoubleComplex b) {
+  acc.x = fma(-a.x, b.x, acc.x); acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(-a.x, b.y, acc.y); acc.y = fma(-a.y, b.x, acc.y);
+}
+
+// Panel solve X = B L^-H in place (L^-T for real types), row-parallel: B (m x jb,
+// jb <= 128, logical view B(i, j) = B[i*brs + j*bcs]) is overwritten by X, and X
+// also goes to out2 (out2[i*o_rs + j*o_cs]; ROUND: rounded to the tensor-core
+// operand type O2, BF16 or TF32, else a plain conversion).  L: the factored jb x jb
+// diagonal block (view strides lrs, lcs).  Each row x of X solves x L^H = b:
+//   x_k = (b_k - sum_{j<k} x_j conj(L(k, j))) / L(k, k),
+// so the block is staged as conj(L).  CTA: 64 rows; thread (r, cg) holds columns
 // [32cg, 32cg + 32) of row r in registers.  Column block b is solved by the threads
 // with cg == b (forward substitution, right-looking inside the block), published
 // through shared memory, and subtracted by the threads with cg > b.  Computes in T.
+// Complex double rows need up to 255 registers: one CTA per SM for that type.
 template <typename T, typename TB, typename TL, typename O2, bool ROUND>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, sizeof(T) == 16 ? 1 : 2)
     trsm_rows_kernel(TB* __restrict__ B, long long brs, long long bcs, int m, int jb, const TL* __restrict__ L,
                      long long lrs, long long lcs, O2* __restrict__ out2, long long o_rs, long long o_cs,
                      const int* __restrict__ stop) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: L(32b + j, 32b + k)
+  T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: conj L(32b + j, 32b + k)
   T* Xs = Ls + 128 * 33;                    // [64][33]: solved block
   T* rd = Xs + 64 * 33;                     // [32]: 1 / L(32b + j, 32b + j)
   if (*stop != 0) return;
@@ -43,7 +65,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
     const int col = cg * 32 + k;
-    x[k] = (row < m && col < jb) ? (T)B[(long long)row * brs + (long long)col * bcs] : T(0);
+    x[k] = (row < m && col < jb) ? cvt<T>(B[(long long)row * brs + (long long)col * bcs]) : zero<T>();
   }
   const int nblk = (jb + 31) / 32;
   for (int b = 0; b < nblk; ++b) {
@@ -52,17 +74,18 @@ __global__ void __launch_bounds__(256, 2)
     for (int e = t; e < rows * 32; e += 256) {
       const int j = e >> 5, kk = e & 31;
       const int gi = 32 * b + j, gk = 32 * b + kk;
-      Ls[j * 33 + kk] = (gi < jb && gk < jb && gi >= gk) ? (T)L[(long long)gi * lrs + (long long)gk * lcs] : T(0);
+      Ls[j * 33 + kk] =
+          (gi < jb && gk < jb && gi >= gk) ? cj(cvt<T>(L[(long long)gi * lrs + (long long)gk * lcs])) : zero<T>();
     }
     __syncthreads();
-    if (t < 32) rd[t] = (32 * b + t < jb) ? T(1) / Ls[t * 33 + t] : T(0);
+    if (t < 32) rd[t] = (32 * b + t < jb) ? recip(Ls[t * 33 + t]) : zero<T>();
     __syncthreads();
     if (cg == b) {
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
-        x[j] *= rd[j];
+        x[j] = mul(x[j], rd[j]);
 #pragma unroll
-        for (int kk = j + 1; kk < 32; ++kk) x[kk] -= Ls[kk * 33 + j] * x[j];
+        for (int kk = j + 1; kk < 32; ++kk) msub(x[kk], Ls[kk * 33 + j], x[j]);
       }
 #pragma unroll
       for (int kk = 0; kk < 32; ++kk) Xs[r * 33 + kk] = x[kk];
@@ -74,7 +97,7 @@ __global__ void __launch_bounds__(256, 2)
       for (int kk = 0; kk < 32; ++kk) {
         const T xk = Xs[r * 33 + kk];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] -= Lb[j * 33 + kk] * xk;
+        for (int j = 0; j < 32; ++j) msub(x[j], Lb[j * 33 + kk], xk);
       }
     }
   }
@@ -83,11 +106,11 @@ __global__ void __launch_bounds__(256, 2)
     for (int k = 0; k < 32; ++k) {
       const int col = cg * 32 + k;
       if (col < jb) {
-        B[(long long)row * brs + (long long)col * bcs] = (TB)x[k];
+        B[(long long)row * brs + (long long)col * bcs] = cvt<TB>(x[k]);
         if constexpr (ROUND) {
           out2[(long long)row * o_rs + (long long)col * o_cs] = to_op<O2>((float)x[k]);
         } else {
-          out2[(long long)row * o_rs + (long long)col * o_cs] = (O2)x[k];
+          out2[(long long)row * o_rs + (long long)col * o_cs] = cvt<O2>(x[k]);
         }
       }
     }
