@@ -19,6 +19,7 @@
 #include "zmma.cuh"
 #include "handle.h"
 #include "panel.cuh"
+#include "tc.cuh"
 #include "trsm.cuh"
 #include "tuning.cuh"
 
@@ -395,6 +396,69 @@ CUresult set_smem(const void* fn, size_t bytes) {
   return CUDA_SUCCESS;
 }
 
+// ---- FP32 updates on the TF32 tensor cores, split in three (tc.cuh, SPLIT3) -------
+// C -= Q(r) Q(c)^T on the logical lower trapezoid m x ncols whose corner is the
+// diagonal element (r0, r0) of A (column-major, lda), with Q = qhi + qlo k-major (row
+// pitch ldq, q_rows rows): operand rows from qrow, k columns [koff, koff + k).  Upper
+// storage (rs = lda) writes the same symmetric update into the physical upper
+// trapezoid.  The caller checks the alignment rules (tc3_usable).
+bool tc3_usable(const float* A, long long lda) { return aligned16(A) && (lda % 4) == 0; }
+
+CUresult tc3_update(CULAPACKhandle h, const float* qhi, const float* qlo, long long ldq, int q_rows, int qrow,
+                    int koff, int k, float* A, long long lda, bool upper, int r0, int m, int ncols, cudaStream_t s,
+                    const int* stop) {
+  if (m <= 0 || ncols <= 0 || k <= 0) return CUDA_SUCCESS;
+  EncodeTiledFn fn = encode_tiled();
+  if (fn == nullptr) return CUDA_ERROR_NOT_SUPPORTED;
+  CUtensorMap mhi, mlo, mc;
+  const cuuint32_t es[2] = {1, 1};
+  const cuuint64_t qdims[2] = {(cuuint64_t)k, (cuuint64_t)q_rows};
+  const cuuint64_t qstr[1] = {(cuuint64_t)ldq * sizeof(float)};
+  const cuuint32_t qbox[2] = {(cuuint32_t)tc::OpKind<float>::BK, (cuuint32_t)tc::BM};
+  for (int w = 0; w < 2; ++w) {
+    const float* q = (w == 0 ? qhi : qlo) + koff;
+    if (fn(w == 0 ? &mhi : &mlo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(q), qdims, qstr, qbox, es,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return CUDA_ERROR_INVALID_VALUE;
+  }
+  float* corner = A + (long long)r0 * (lda + 1);
+  const cuuint64_t cdims[2] = {(cuuint64_t)(upper ? ncols : m), (cuuint64_t)(upper ? m : ncols)};
+  const cuuint64_t cstr[1] = {(cuuint64_t)lda * sizeof(float)};
+  const cuuint32_t cbox[2] = {32, 32};
+  if (fn(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, corner, cdims, cstr, cbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         upper ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return CUDA_ERROR_INVALID_VALUE;
+  tc::Params prm{};
+  prm.m = m;
+  prm.n = ncols;
+  prm.k = k;
+  prm.a_row0 = qrow;
+  prm.b_row0 = qrow;
+  prm.alpha = -1.f;
+  prm.lower_only = 1;
+  prm.tiles_m = (m + tc::BM - 1) / tc::BM;
+  prm.tiles_n = (ncols + tc::BN - 1) / tc::BN;
+  prm.err = h->d_words + 3;
+  const int tiles = prm.tiles_n * (prm.tiles_n + 1) / 2 + (prm.tiles_m - prm.tiles_n) * prm.tiles_n;
+  constexpr int smem = tc::Ring<true>::SMEM;
+  static bool attr[2] = {false, false};
+  if (!attr[upper]) {
+    CUCHOL_CHECK(cudaFuncSetAttribute(upper ? (const void*)tc::update_kernel<float, true, true>
+                                            : (const void*)tc::update_kernel<float, true, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr[upper] = true;
+  }
+  if (upper)
+    tc::update_kernel<float, true, true><<<tiles, tc::THREADS, smem, s>>>(mhi, mlo, mc, prm, stop);
+  else
+    tc::update_kernel<float, true, false><<<tiles, tc::THREADS, smem, s>>>(mhi, mlo, mc, prm, stop);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
 // ---- ?POTRF ---------------------------------------------------------------------
 // Right-looking blocked Cholesky, outer blocks of NB = sub*nb columns (each factored
 // as sub nb-wide sub-panels; sub from the tuning table, 2 to 8 by n for FP64),
@@ -437,14 +501,24 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   int* d_info = h->d_words;
 
   const long long ldp = (long long)round_up((size_t)n, 2);
-  const size_t ws = sizeof(T) * (2 * (size_t)ldp * NB);
+  // FP32 with an aligned A: the updates run on the TF32 tensor cores as split
+  // products, from hi / lo copies of the solved panel in k-major buffers Q (row
+  // r = P row r, pitch ldq), ping-pong like P; P itself is then not needed
+  bool tc3 = false;
+  if constexpr (std::is_same<T, float>::value) tc3 = !h->force_simt && tc3_usable(A, lda) && n > 128;
+  const long long ldq = (long long)round_up((size_t)NB, 32);
+  const size_t ws = tc3 ? sizeof(T) * 4 * (size_t)n * ldq : sizeof(T) * (2 * (size_t)ldp * NB);
   CUCHOL_CHECK_CU(ensure_workspace(h, ws));
   T* pbuf[2] = {static_cast<T*>(h->ws), static_cast<T*>(h->ws) + (size_t)ldp * NB};
+  T* qbuf[4] = {static_cast<T*>(h->ws), static_cast<T*>(h->ws) + (size_t)n * ldq,
+                static_cast<T*>(h->ws) + 2 * (size_t)n * ldq, static_cast<T*>(h->ws) + 3 * (size_t)n * ldq};
 
   CUCHOL_CHECK_CU(set_smem<T>((const void*)diag_factor_kernel<T, nb, kDiagThreads2>, Smem::bytes));
   // the panel solve is a row-parallel triangular solve (no inverse of the diagonal
   // block) that writes the solved rows into A and into P
-  CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, false>, trsm_rows_smem<T>()));
+  CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, OUT_CONVERT>, trsm_rows_smem<T>()));
+  if constexpr (std::is_same<T, float>::value)
+    CUCHOL_CHECK_CU(set_smem<T>((const void*)trsm_rows_kernel<T, T, T, T, OUT_SPLIT>, trsm_rows_smem<T>()));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
   CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
   // the update stream starts after the panel stream's initialisation
@@ -453,13 +527,19 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
   CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
 
   const T minus_one = from_real<T>(RealOf<T>(-1)), one = from_real<T>(RealOf<T>(1));
-  // C -= Ahat Bhat^H on a lower-only view of A at (r0, c0), operands rows of P
-  auto update = [&](long long r0, long long c0, int m, int ncols, const T* pa, const T* pb, int k,
+  // C -= Phat Phat^H on the lower trapezoid m x ncols of A with its corner on the
+  // diagonal at r0; operand rows from P row prow (both sides), k columns [koff, koff + k)
+  auto update = [&](const T* P, const T* Qh, const T* Ql, int r0, int m, int ncols, int prow, int koff, int k,
                     cudaStream_t s) -> CUresult {
+    if constexpr (std::is_same<T, float>::value) {
+      if (tc3)
+        return tc3_update(h, Qh, Ql, ldq, n, prow, koff, k, A, lda, upper, r0, m, ncols, s, d_info);
+    }
+    const T* pa = P + prow + (long long)koff * ldp;
     GemmProblem<T> u = problem<T>();
     u.a = pa; u.a_rs = 1; u.a_ks = ldp;
-    u.b = pb; u.b_rs = 1; u.b_ks = ldp; u.conj_b = 1;
-    u.c = at(r0, c0); u.c_rs = rs; u.c_cs = cs;
+    u.b = pa; u.b_rs = 1; u.b_ks = ldp; u.conj_b = 1;
+    u.c = at(r0, r0); u.c_rs = rs; u.c_cs = cs;
     u.cin = u.c; u.cin_rs = rs; u.cin_cs = cs;
     u.alpha = minus_one; u.beta = one;
     u.lower_only = 1; u.real_diag = 1;
@@ -472,6 +552,8 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
     const int m = n - j - jB;                    // rows below the outer block
     const int mc = ncols - j - jB;               // columns right of it (in the panel)
     T* P = pbuf[step & 1];
+    T* Qh = qbuf[2 * (step & 1)];
+    T* Ql = qbuf[2 * (step & 1) + 1];
     for (int s0 = 0; s0 < jB; s0 += nb) {
       const int c = j + s0, jb = std::min(nb, j + jB - c);
       const int mr = n - c - jb;                 // rows below this diagonal block
@@ -484,31 +566,43 @@ CUresult potrf_run(CULAPACKhandle h, bool upper, int n, T* A, long long lda, lon
         break;
       }
       // panel solve into P: rows c + jb .. n-1 are P rows s0 .. (P starts at j + nb)
-      T* Ps = P + s0 + (long long)s0 * ldp;
-      // row-parallel triangular solve: A21 := A21 L11^-H in place, and into P
-      trsm_rows_kernel<T, T, T, T, false><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
-          at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
+      // row-parallel triangular solve: A21 := A21 L11^-H in place, and into P (or its
+      // hi / lo split into Q)
+      bool split = false;
+      if constexpr (std::is_same<T, float>::value) {
+        if (tc3) {
+          const long long qo = (long long)s0 * ldq + s0;
+          trsm_rows_kernel<T, T, T, T, OUT_SPLIT><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
+              at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Qh + qo, ldq, 1, d_info, Ql + qo);
+          split = true;
+        }
+      }
+      if (!split) {
+        T* Ps = P + s0 + (long long)s0 * ldp;
+        trsm_rows_kernel<T, T, T, T, OUT_CONVERT><<<(mr + 63) / 64, 256, trsm_rows_smem<T>(), sp>>>(
+            at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info, nullptr);
+      }
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       CUCHOL_CHECK(cudaEventRecord(h->ev_panel, sp));
       if (on_final) CUCHOL_CHECK_CU((*on_final)(c, jb, sp));
       if (s0 + nb < jB) {
-        // the outer block's remaining sub-panel columns (rows c + nb ..) by this one
-        const T* Pc = P + s0 + (long long)s0 * ldp;
-        CUCHOL_CHECK_CU(update(c + nb, c + nb, n - c - nb, jB - s0 - nb, Pc, Pc, nb, sp));
+        // the outer block's remaining sub-panel columns (rows c + nb .., P rows s0 ..)
+        // by this one (k columns s0 .. s0 + nb)
+        CUCHOL_CHECK_CU(update(P, Qh, Ql, c + nb, n - c - nb, jB - s0 - nb, s0, s0, nb, sp));
       }
     }
     if (m == 0 || mc == 0) break;
     // lookahead: next outer block (P rows from j + NB, k = jB), after the previous
     // trailing update
     const int jB2 = std::min(NB, mc);
-    const T* Pt = P + (NB - nb);
+    const int pt = NB - nb;              // P row of global row j + NB
     CUCHOL_CHECK(cudaStreamWaitEvent(sp, h->ev_update, 0));
-    CUCHOL_CHECK_CU(update(j + NB, j + NB, m, jB2, Pt, Pt, jB, sp));
+    CUCHOL_CHECK_CU(update(P, Qh, Ql, j + NB, m, jB2, pt, 0, jB, sp));
     // rest of the trailing matrix, once P holds both sub-panels
     CUCHOL_CHECK(cudaStreamWaitEvent(su, h->ev_panel, 0));
     if (mc > jB2)
-      CUCHOL_CHECK_CU(update(j + NB + jB2, j + NB + jB2, m - jB2, mc - jB2, Pt + jB2, Pt + jB2, jB, su));
+      CUCHOL_CHECK_CU(update(P, Qh, Ql, j + NB + jB2, m - jB2, mc - jB2, pt + jB2, 0, jB, su));
     // always recorded: it also covers the copies that still read P
     CUCHOL_CHECK(cudaEventRecord(h->ev_update, su));
   }

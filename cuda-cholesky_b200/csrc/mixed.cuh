@@ -1141,7 +1141,7 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* in
   Op* Q[2] = {reinterpret_cast<Op*>(ws + small), reinterpret_cast<Op*>(ws + small + qbytes)};
   static bool attr = false;
   if (!attr) {
-    CUCHOL_CHECK(cudaFuncSetAttribute(trsm_rows_kernel<float, float, double, Op, true>,
+    CUCHOL_CHECK(cudaFuncSetAttribute(trsm_rows_kernel<float, float, double, Op, OUT_ROUND>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_rows_smem<float>()));
     attr = true;
   }
@@ -1170,8 +1170,8 @@ CUresult mixed_factor(CULAPACKhandle h, int n, float* W, long long ldw, long* in
       if (mr == 0) break;
       // panel rows c + jb .. n-1 solved in place; they are Q rows s0 .., columns s0 ..
       Op* Qs = Qj + (long long)s0 * ldq + s0;
-      trsm_rows_kernel<float, float, double, Op, true><<<(mr + 63) / 64, kThreads, trsm_rows_smem<float>(), sp>>>(
-          at(c + jb, c), 1, ldw, mr, jb, D, 1, SB, Qs, ldq, 1, d_info);
+      trsm_rows_kernel<float, float, double, Op, OUT_ROUND><<<(mr + 63) / 64, kThreads, trsm_rows_smem<float>(), sp>>>(
+          at(c + jb, c), 1, ldw, mr, jb, D, 1, SB, Qs, ldq, 1, d_info, nullptr);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (s0 + SB < jB)   // the outer block's remaining columns by this sub-panel

@@ -72,7 +72,7 @@ CUresult potrf_ozaki_run(CULAPACKhandle h, bool upper, int n, double* A, long lo
                   reinterpret_cast<int*>(ws + pbytes + 2 * sbytes + ebytes)};
 
   CUCHOL_CHECK_CU(set_smem<double>((const void*)diag_factor_kernel<double, nb, kDiagThreads2>, Smem::bytes));
-  CUCHOL_CHECK_CU(set_smem<double>((const void*)trsm_rows_kernel<double, double, double, double, false>,
+  CUCHOL_CHECK_CU(set_smem<double>((const void*)trsm_rows_kernel<double, double, double, double, OUT_CONVERT>,
                                    trsm_rows_smem<double>()));
   CUCHOL_CHECK(cudaMemsetAsync(d_info, 0, sizeof(int), sp));
   CUCHOL_CHECK(cudaMemsetAsync(h->d_logdet, 0, sizeof(double), sp));
@@ -93,8 +93,8 @@ CUresult potrf_ozaki_run(CULAPACKhandle h, bool upper, int n, double* A, long lo
       CUCHOL_CHECK(cudaGetLastError());
       if (mr == 0) break;
       double* Ps = P + s0 + (long long)s0 * ldp;   // P(r, .) = rows from j + nb
-      trsm_rows_kernel<double, double, double, double, false><<<(mr + 63) / 64, 256, trsm_rows_smem<double>(), sp>>>(
-          at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info);
+      trsm_rows_kernel<double, double, double, double, OUT_CONVERT><<<(mr + 63) / 64, 256, trsm_rows_smem<double>(), sp>>>(
+          at(c + jb, c), rs, cs, mr, jb, at(c, c), rs, cs, Ps, 1, ldp, d_info, nullptr);
       ++h->launches;
       CUCHOL_CHECK(cudaGetLastError());
       if (s0 + nb < jB) {   // the outer block's remaining sub-panel columns by this one (DMMA)

@@ -192,11 +192,31 @@ __device__ __forceinline__ void tile_of(int t, const Params& p, int& ti, int& tj
   }
 }
 
-template <typename Op>
-__global__ void __launch_bounds__(THREADS, 2)
+// SPLIT3 (TF32 only): FP32 products to about FP32 accuracy on the TF32 tensor cores.
+// Every operand is held as hi = tf32(x) and lo = tf32(x - hi) (x = hi + lo to
+// 2^-22 |x|), ma maps the hi values and mb the lo values of one k-major matrix Q
+// (A rows from a_row0, B rows from b_row0 of both), and each k block issues
+//     lo_A hi_B^T + hi_A lo_B^T + hi_A hi_B^T
+// into the same FP32 accumulator (the dropped lo lo^T term is below 2^-22 of the
+// product).  A stage then holds four 16 KB tiles, so one CTA per SM.
+// UPPER: the region (described, like the lower case, as the logical lower trapezoid
+// m x n with its corner on the diagonal) is stored transposed: mc maps the physical
+// n x m upper trapezoid of a column-major matrix (the symmetric update of upper
+// storage), with a 128-byte swizzle, and each 32 x 32 block is staged transposed.
+template <bool SPLIT3> struct Ring {
+  static constexpr int STAGE = SPLIT3 ? 2 * (A_STAGE + B_STAGE) : A_STAGE + B_STAGE;
+  static constexpr int SMEM = STAGES * STAGE + 1024;
+  static constexpr int A_OFF_LO = A_STAGE;                       // SPLIT3 layout: Ahi Alo Bhi Blo
+  static constexpr int B_OFF = SPLIT3 ? 2 * A_STAGE : A_STAGE;
+};
+
+template <typename Op, bool SPLIT3 = false, bool UPPER = false>
+__global__ void __launch_bounds__(THREADS, SPLIT3 ? 1 : 2)
     update_kernel(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
                   const __grid_constant__ CUtensorMap mc, Params p, const int* stop) {
+  static_assert(!SPLIT3 || sizeof(Op) == 4, "the split product is for TF32 operands");
   constexpr int BK = OpKind<Op>::BK;
+  using RG = Ring<SPLIT3>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full[STAGES];
   __shared__ __align__(8) uint64_t empty[STAGES];
@@ -237,10 +257,17 @@ __global__ void __launch_bounds__(THREADS, 2)
         s_fail = 1;
         break;
       }
-      uint8_t* st = base + s * STAGE_BYTES;
-      mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_2d(&ma, &full[s], st, kb * BK, p.a_row0 + row0);
-      tma_load_2d(&mb, &full[s], st + A_STAGE, kb * BK, p.b_row0 + col0);
+      uint8_t* st = base + s * RG::STAGE;
+      mbar_expect_tx(&full[s], RG::STAGE);
+      if constexpr (SPLIT3) {
+        tma_load_2d(&ma, &full[s], st, kb * BK, p.a_row0 + row0);
+        tma_load_2d(&mb, &full[s], st + RG::A_OFF_LO, kb * BK, p.a_row0 + row0);
+        tma_load_2d(&ma, &full[s], st + RG::B_OFF, kb * BK, p.b_row0 + col0);
+        tma_load_2d(&mb, &full[s], st + RG::B_OFF + B_STAGE, kb * BK, p.b_row0 + col0);
+      } else {
+        tma_load_2d(&ma, &full[s], st, kb * BK, p.a_row0 + row0);
+        tma_load_2d(&mb, &full[s], st + RG::B_OFF, kb * BK, p.b_row0 + col0);
+      }
       ++issued;
     }
   } else if (threadIdx.x == 32) {
@@ -253,10 +280,18 @@ __global__ void __launch_bounds__(THREADS, 2)
         break;
       }
       fence_after();
-      const uint32_t a = smem_u32(base + s * STAGE_BYTES), b = a + A_STAGE;
+      const uint32_t a = smem_u32(base + s * RG::STAGE), b = a + RG::B_OFF;
 #pragma unroll
-      for (int kk = 0; kk < ROW_BYTES / 32; ++kk)
-        mma<Op>(tmem, smem_desc(a + 32 * kk), smem_desc(b + 32 * kk), (kb | kk) != 0 ? 1u : 0u);
+      for (int kk = 0; kk < ROW_BYTES / 32; ++kk) {
+        if constexpr (SPLIT3) {
+          const uint32_t alo = a + RG::A_OFF_LO, blo = b + B_STAGE;
+          mma<Op>(tmem, smem_desc(alo + 32 * kk), smem_desc(b + 32 * kk), (kb | kk) != 0 ? 1u : 0u);
+          mma<Op>(tmem, smem_desc(a + 32 * kk), smem_desc(blo + 32 * kk), 1u);
+          mma<Op>(tmem, smem_desc(a + 32 * kk), smem_desc(b + 32 * kk), 1u);
+        } else {
+          mma<Op>(tmem, smem_desc(a + 32 * kk), smem_desc(b + 32 * kk), (kb | kk) != 0 ? 1u : 0u);
+        }
+      }
       mma_commit(&empty[s]);
     }
     s_consumed = kb;
@@ -289,12 +324,26 @@ __global__ void __launch_bounds__(THREADS, 2)
       }
       float v[32];
       tmem_ld32(trow + 32 * cc, v);
+      if constexpr (UPPER) {
+        // transposed block: physical column = this lane's row, 128-byte swizzled rows
 #pragma unroll
-      for (int i = 0; i < 32; ++i) buf[i * 32 + lane] = (!p.lower_only || r >= cbase + i) ? p.alpha * v[i] : 0.f;
+        for (int q = 0; q < 8; ++q) {
+          float4 w;
+          w.x = (!p.lower_only || r >= cbase + 4 * q + 0) ? p.alpha * v[4 * q + 0] : 0.f;
+          w.y = (!p.lower_only || r >= cbase + 4 * q + 1) ? p.alpha * v[4 * q + 1] : 0.f;
+          w.z = (!p.lower_only || r >= cbase + 4 * q + 2) ? p.alpha * v[4 * q + 2] : 0.f;
+          w.w = (!p.lower_only || r >= cbase + 4 * q + 3) ? p.alpha * v[4 * q + 3] : 0.f;
+          *reinterpret_cast<float4*>(buf + lane * 32 + ((q ^ (lane & 7)) << 2)) = w;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) buf[i * 32 + lane] = (!p.lower_only || r >= cbase + i) ? p.alpha * v[i] : 0.f;
+      }
       fence_proxy_async();
       __syncwarp();
       if (lane == 0) {
-        tma_reduce_add_2d(&mc, buf, row0 + 32 * warp, cbase);
+        if constexpr (UPPER) tma_reduce_add_2d(&mc, buf, cbase, row0 + 32 * warp);
+        else tma_reduce_add_2d(&mc, buf, row0 + 32 * warp, cbase);
         bulk_commit();
       }
     }

@@ -38,10 +38,17 @@ __device__ __forceinline__ void msub(cuDoubleComplex& acc, cuDoubleComplex a, cu
   acc.y = fma(-a.x, b.y, acc.y); acc.y = fma(-a.y, b.x, acc.y);
 }
 
+// How the panel solve writes its second copy of X (out2, and out3 for the split).
+enum : int {
+  OUT_CONVERT = 0,   // out2 = X converted to O2
+  OUT_ROUND = 1,     // out2 = X rounded to the tensor-core operand type O2 (BF16 or TF32)
+  OUT_SPLIT = 2,     // out2 = hi = tf32(X), out3 = lo = tf32(X - hi): X = hi + lo to 2^-22
+};
+
 // Panel solve X = B L^-H in place (L^-T for real types), row-parallel: B (m x jb,
 // jb <= 128, logical view B(i, j) = B[i*brs + j*bcs]) is overwritten by X, and X
-// also goes to out2 (out2[i*o_rs + j*o_cs]; ROUND: rounded to the tensor-core
-// operand type O2, BF16 or TF32, else a plain conversion).  L: the factored jb x jb
+// also goes to out2 (out2[i*o_rs + j*o_cs]) and, for OUT_SPLIT, out3 (same strides),
+// as MODE says.  L: the factored jb x jb
 // diagonal block (view strides lrs, lcs).  Each row x of X solves x L^H = b:
 //   x_k = (b_k - sum_{j<k} x_j conj(L(k, j))) / L(k, k),
 // so the block is staged as conj(L).  CTA: 64 rows; thread (r, cg) holds columns
@@ -49,11 +56,11 @@ __device__ __forceinline__ void msub(cuDoubleComplex& acc, cuDoubleComplex a, cu
 // with cg == b (forward substitution, right-looking inside the block), published
 // through shared memory, and subtracted by the threads with cg > b.  Computes in T.
 // Complex double rows need up to 255 registers: one CTA per SM for that type.
-template <typename T, typename TB, typename TL, typename O2, bool ROUND>
+template <typename T, typename TB, typename TL, typename O2, int MODE>
 __global__ void __launch_bounds__(256, sizeof(T) == 16 ? 1 : 2)
     trsm_rows_kernel(TB* __restrict__ B, long long brs, long long bcs, int m, int jb, const TL* __restrict__ L,
                      long long lrs, long long lcs, O2* __restrict__ out2, long long o_rs, long long o_cs,
-                     const int* __restrict__ stop) {
+                     const int* __restrict__ stop, O2* __restrict__ out3) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: conj L(32b + j, 32b + k)
   T* Xs = Ls + 128 * 33;                    // [64][33]: solved block
@@ -107,10 +114,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 16 ? 1 : 2)
       const int col = cg * 32 + k;
       if (col < jb) {
         B[(long long)row * brs + (long long)col * bcs] = cvt<TB>(x[k]);
-        if constexpr (ROUND) {
-          out2[(long long)row * o_rs + (long long)col * o_cs] = to_op<O2>((float)x[k]);
+        const long long o = (long long)row * o_rs + (long long)col * o_cs;
+        if constexpr (MODE == OUT_ROUND) {
+          out2[o] = to_op<O2>((float)x[k]);
+        } else if constexpr (MODE == OUT_SPLIT) {
+          const float hi = round_tf32((float)x[k]);
+          out2[o] = hi;
+          out3[o] = round_tf32((float)x[k] - hi);
         } else {
-          out2[(long long)row * o_rs + (long long)col * o_cs] = cvt<O2>(x[k]);
+          out2[o] = cvt<O2>(x[k]);
         }
       }
     }

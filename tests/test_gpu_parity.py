@@ -251,18 +251,22 @@ def test_outer_block_sizes(handle, p, u):
     from cucholesky import tune
     lib = cc.lib()
     tune._declare(lib)
-    n, lda = 2200, 2203
-    A = matgen.spd(p, n, seed=5, lda=lda)
-    Fo = A.copy(order="F")
-    assert O.potrf(p, u, Fo, lda=lda) == 0
+    n = 2200
+    # lda = n + 3 takes the general engines; for FP32, lda = n (16-byte rows) takes the
+    # split TF32 tensor-core updates
+    ldas = (n + 3, n) if p == "s" else (n + 3,)
     try:
-        for sub in (1, 2, 3, 4, 5, 6, 8, 12, 16):
-            assert lib.cuLAPACKSetPotrfBlocks(handle.value, sub) == 0
-            F, info = gpu_call(handle, "potrf", p, u, A)
-            assert info == 0
-            assert matgen.backward_error(A, F, u) <= 10, sub
-            d = np.abs(_tri(u)(F[:n, :n] - Fo[:n, :n])).max()
-            assert d <= 50 * n * EPS[p] * np.abs(A[:n, :n]).max(), (sub, d)
+        for lda in ldas:
+            A = matgen.spd(p, n, seed=5, lda=lda)
+            Fo = A.copy(order="F")
+            assert O.potrf(p, u, Fo, lda=lda) == 0
+            for sub in (1, 2, 3, 4, 5, 6, 8, 12, 16):
+                assert lib.cuLAPACKSetPotrfBlocks(handle.value, sub) == 0
+                F, info = gpu_call(handle, "potrf", p, u, A)
+                assert info == 0
+                assert matgen.backward_error(A, F, u) <= 10, (lda, sub)
+                d = np.abs(_tri(u)(F[:n, :n] - Fo[:n, :n])).max()
+                assert d <= 50 * n * EPS[p] * np.abs(A[:n, :n]).max(), (lda, sub, d)
     finally:
         assert lib.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
     v = C.c_int(0)
