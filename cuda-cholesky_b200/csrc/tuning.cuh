@@ -34,10 +34,12 @@ struct TuneRow {
 
 // FP64 ?potrf, B200: outer blocks of 2 / 3 / 4 / 6 / 8 diagonal blocks, measured at
 // n = 4096 / 8192 / 16384 / 32768 (best 4.25, 11.22, 56.55, 398.1 ms) and split at the
-// geometric midpoints.  S, C, Z: the rows tune.py wrote from n = 4096 / 8192 / 16384
-// (best spotrf 3.93 / 14.27 / 87.34 ms, cpotrf 7.34 / 29.82 / 196.8 ms; outer block 2
-// gave 93.65 and 208.5 ms at n = 16384).  Z on the complex FP64 tensor-core engine:
-// best 9.93 / 37.56 / 223.9 ms with 2 / 6 / 12 (outer block 2 gave 293.5 ms at 16384).
+// geometric midpoints.  C: the rows tune.py wrote from n = 4096 / 8192 / 16384 (best
+// cpotrf 7.34 / 29.82 / 196.8 ms; outer block 2 gave 208.5 ms at n = 16384).  Z on
+// the complex FP64 tensor-core engine: best 9.93 / 37.56 / 223.9 ms with 2 / 6 / 12
+// (outer block 2 gave 293.5 ms at 16384).  S on the split TF32 tensor-core updates:
+// flat in the width up to n = 8192 (2.78 / 6.09 ms), best 4 at 16384 (16.69 ms; 1
+// gave 22.37) and within 1% of the best at 32768 (88.74 ms).
 // cuDpotrfOzaki: 8 (1024 columns) below n = 49152, 16 from there on (n = 8192 / 32768 /
 // 65536: 10.8 / 255 / 2028 ms with 8; 11.7 / 255 / 1926 ms with 16; 4 gave 282 ms and
 // 2344 ms at the two larger orders).
@@ -45,7 +47,7 @@ inline std::vector<TuneRow>& tuning_rows() {
   static std::vector<TuneRow> rows = {
       {TUNE_POTRF, 'D', 0, 2}, {TUNE_POTRF, 'D', 6144, 3}, {TUNE_POTRF, 'D', 12288, 4},
       {TUNE_POTRF, 'D', 24576, 6}, {TUNE_POTRF, 'D', 49152, 8},
-      {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'S', 5793, 3}, {TUNE_POTRF, 'S', 11585, 8},
+      {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'S', 11585, 4},
       {TUNE_POTRF, 'C', 0, 2}, {TUNE_POTRF, 'C', 5793, 3}, {TUNE_POTRF, 'C', 11585, 6},
       {TUNE_POTRF, 'Z', 0, 2}, {TUNE_POTRF, 'Z', 5793, 6}, {TUNE_POTRF, 'Z', 11585, 12},
       {TUNE_OZAKI, 'D', 0, 8}, {TUNE_OZAKI, 'D', 49152, 16},

@@ -274,7 +274,7 @@ def test_tuning_table_file(tmp_path):
         restore = tmp_path / "builtin.tuning"
         lines = ["cucholesky-tuning 1"]
         lines += ["potrf D 0 2", "potrf D 6144 3", "potrf D 12288 4", "potrf D 24576 6", "potrf D 49152 8",
-                  "potrf S 0 2", "potrf S 5793 3", "potrf S 11585 8", "potrf C 0 2", "potrf C 5793 3",
+                  "potrf S 0 2", "potrf S 11585 4", "potrf C 0 2", "potrf C 5793 3",
                   "potrf C 11585 6", "potrf Z 0 2", "potrf Z 5793 6", "potrf Z 11585 12", "ozaki D 0 8", "ozaki D 49152 16"]
         restore.write_text("\n".join(lines) + "\n")
         assert lib.cuLAPACKLoadTuning(str(restore).encode()) == 0
