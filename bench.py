@@ -84,8 +84,10 @@ def parse():
                     help="potrf: the default line; batched / mixed / ozaki: that target as its own line")
     ap.add_argument("--dtype", default="d", choices=["d", "s"], help="batched workload precision")
     ap.add_argument("--syrk", nargs=2, type=int, metavar=("M", "K"),
-                    help="only the dominant kernel: two cuDsyrk(L, N) launches of order M, rank K "
-                         "(warm-up + measured), for profiling")
+                    help="only the dominant kernel: two cu?syrk / cu?herk(L, N) launches of order M, "
+                         "rank K (warm-up + measured), for profiling")
+    ap.add_argument("--syrk-type", default="D", choices=["D", "Z"],
+                    help="--syrk element type: D (cuDsyrk) or Z (cuZherk)")
     ap.add_argument("--syrk-lowp", nargs=3, metavar=("M", "K", "PREC"),
                     help="only the mixed factor's trailing update: two cuSsyrkLowp launches of order M, "
                          "rank K, PREC bf16 or tf32 (warm-up + measured), for profiling")
@@ -743,18 +745,20 @@ def ozaki_result(torch, cc, n, peak):
 # ---------------------------------------------------------------------------------
 # single-kernel modes (profiling)
 # ---------------------------------------------------------------------------------
-def run_syrk_only(m: int, k: int) -> None:
+def run_syrk_only(m: int, k: int, prefix: str = "D") -> None:
     import torch
     import cucholesky as cc
+    dt = torch.float64 if prefix == "D" else torch.complex128
     bh = cc.BlasHandle()
-    P = torch.randn(k, m, dtype=torch.float64, device="cuda")     # column-major m x k
-    C = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    P = torch.randn(k, m, dtype=dt, device="cuda")     # column-major m x k
+    C = torch.zeros(m, m, dtype=dt, device="cuda")
     st = torch.cuda.current_stream()
+    mult = 4 if prefix == "Z" else 1
     for _ in range(2):
-        ms, rc = timed(torch, lambda: cc.call_rankk(bh, "D", "L", "N", m, k, -1.0, P.data_ptr(), m, 1.0,
+        ms, rc = timed(torch, lambda: cc.call_rankk(bh, prefix, "L", "N", m, k, -1.0, P.data_ptr(), m, 1.0,
                                                      C.data_ptr(), m, st.cuda_stream), st)
-        print(json.dumps({"kernel": "cuDsyrk L,N", "m": m, "k": k, "rc": rc, "ms": ms,
-                          "tflops": float(m) * (m + 1) * k / (ms / 1e3) / 1e12}), flush=True)
+        print(json.dumps({"kernel": "cuDsyrk L,N" if prefix == "D" else "cuZherk L,N", "m": m, "k": k, "rc": rc,
+                          "ms": ms, "tflops": mult * float(m) * (m + 1) * k / (ms / 1e3) / 1e12}), flush=True)
     bh.close()
 
 
@@ -969,7 +973,7 @@ def main():
         args.n = N_DEFAULT
     rank, world, local = dist_env()
     if args.syrk:
-        run_syrk_only(*args.syrk)
+        run_syrk_only(args.syrk[0], args.syrk[1], args.syrk_type)
         return
     if args.syrk_lowp:
         run_syrk_lowp_only(int(args.syrk_lowp[0]), int(args.syrk_lowp[1]), args.syrk_lowp[2])

@@ -55,7 +55,7 @@ V* upload(CUcholBatched p, const std::vector<V>& v, CUresult* rc) {
   if (v.empty()) return nullptr;
   if (p->reuse) return static_cast<V*>(p->d_lists[p->cursor++]);   // same order as pass 1
   void* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, v.size() * sizeof(V));
+  cudaError_t e = dev_malloc(&d, v.size() * sizeof(V));
   if (e == cudaSuccess) e = cudaMemcpy(d, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     *rc = report(e, "upload", __func__, __FILE__, __LINE__);
@@ -308,9 +308,9 @@ CUresult tune_nb(CUcholBatched p, const BatchedShape<T>& sh, int* best_nb) {
       cudaFree(d_n);
     }
   } res;
-  CUCHOL_CHECK(cudaMalloc(&res.scratch, sizeof(T) * std::max<long long>(total, 1)));
-  CUCHOL_CHECK(cudaMalloc(&res.d_off, sizeof(long long) * sh.batch));
-  CUCHOL_CHECK(cudaMalloc(&res.d_n, sizeof(int) * sh.batch));
+  CUCHOL_CHECK(dev_malloc(&res.scratch, sizeof(T) * std::max<long long>(total, 1)));
+  CUCHOL_CHECK(dev_malloc(&res.d_off, sizeof(long long) * sh.batch));
+  CUCHOL_CHECK(dev_malloc(&res.d_n, sizeof(int) * sh.batch));
   CUCHOL_CHECK(cudaMemcpy(res.d_off, off.data(), sizeof(long long) * sh.batch, cudaMemcpyHostToDevice));
   CUCHOL_CHECK(cudaMemcpy(res.d_n, sh.n.data(), sizeof(int) * sh.batch, cudaMemcpyHostToDevice));
   T* scratch = res.scratch;
@@ -399,10 +399,10 @@ CUresult batched_create(CUcholBatched* out, CULAPACKhandle h, char type, CBlasUp
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem::bytes) != cudaSuccess ||
       cudaFuncSetAttribute(diag_invert_batched_kernel<T, kBatchedMaxNb, kDiagThreads2>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem::bytes) != cudaSuccess ||
-      cudaMalloc(&p->d_info, sizeof(int) * batch) != cudaSuccess ||
-      cudaMalloc(&p->d_logdet, sizeof(double) * batch) != cudaSuccess ||
-      cudaMalloc(&p->d_w, sizeof(T) * (size_t)batch * kBatchedMaxNb * kBatchedMaxNb) != cudaSuccess ||
-      cudaMalloc(&p->d_work, sizeof(T) * std::max<size_t>(work, 1)) != cudaSuccess)
+      dev_malloc(&p->d_info, sizeof(int) * batch) != cudaSuccess ||
+      dev_malloc(&p->d_logdet, sizeof(double) * batch) != cudaSuccess ||
+      dev_malloc(&p->d_w, sizeof(T) * (size_t)batch * kBatchedMaxNb * kBatchedMaxNb) != cudaSuccess ||
+      dev_malloc(&p->d_work, sizeof(T) * std::max<size_t>(work, 1)) != cudaSuccess)
     return fail(report(cudaGetLastError(), "cudaMalloc", __func__, __FILE__, __LINE__));
   if (nb == 0) {
     rc = tune_nb<T>(p, sh, &nb);

@@ -28,6 +28,8 @@ struct __culapackhandle_st {
   int num_sms;
   unsigned long long launches;   // kernels launched by this handle
   int force_simt;                // testing: route FP64 products to the SIMT engine
+  int wait_limit;                // testing: iterations of the triangular solves' ticket waits
+                                 // (< 0: the default limit)
   int potrf_sub;                 // ?potrf outer block in diagonal blocks (0: tuning table)
   int lauum_cols;                // testing: ?lauum block-column width (0: from the workspace cap)
 };
@@ -43,6 +45,15 @@ inline CUresult to_cu(cudaError_t e) { return static_cast<CUresult>(static_cast<
 const char* error_string(int e);
 
 CUresult report(cudaError_t e, const char* call, const char* func, const char* file, int line);
+
+// Every device allocation of the library (cudaMalloc) goes through here, so that a
+// test can make one fail (cuLAPACKFailAllocation) and check that each
+// routine reports CUDA_ERROR_OUT_OF_MEMORY and leaves its handle usable.
+cudaError_t dev_malloc_bytes(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
 
 // Grow the handle's workspace to at least `bytes` (synchronises the handle's
 // streams first, because queued work may still use the old buffer).

@@ -86,7 +86,7 @@ CUresult stage_buffer(CUmultiGPULAPACKhandle hh, size_t bytes) {
     hh->buf = nullptr;
     hh->buf_bytes = 0;
   }
-  CUCHOL_CHECK(cudaMalloc(&hh->buf, bytes));
+  CUCHOL_CHECK(dev_malloc(&hh->buf, bytes));
   hh->buf_bytes = bytes;
   return CUDA_SUCCESS;
 }

@@ -5,6 +5,7 @@
 // (i, j) of the logical lower triangle at A[i*rs + j*cs], (rs, cs) = (lda, 1)), which
 // produces U = L^T in place; see diag.cuh.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +47,23 @@ namespace cuchol {
 
 const char* error_string(int e) { return cudaGetErrorString(static_cast<cudaError_t>(e)); }
 
+// Allocations still to succeed before one fails (< 0: none fails).
+static std::atomic<int> g_fail_after{-1};
+
+cudaError_t dev_malloc_bytes(void** p, size_t bytes) {
+  int left = g_fail_after.load();
+  while (left >= 0) {
+    if (g_fail_after.compare_exchange_weak(left, left - 1)) {
+      if (left == 0) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+      }
+      break;
+    }
+  }
+  return cudaMalloc(p, bytes);
+}
+
 CUresult report(cudaError_t e, const char* call, const char* func, const char* file, int line) {
   if (errorHandler != nullptr) errorHandler(call, func, file, line, (int)e, &error_string);
   return to_cu(e);
@@ -58,7 +76,7 @@ CUresult ensure_workspace(CULAPACKhandle h, size_t bytes) {
   if (h->ws != nullptr) CUCHOL_CHECK(cudaFree(h->ws));
   h->ws = nullptr;
   h->ws_bytes = 0;
-  CUCHOL_CHECK(cudaMalloc(&h->ws, bytes));
+  CUCHOL_CHECK(dev_malloc(&h->ws, bytes));
   h->ws_bytes = bytes;
   return CUDA_SUCCESS;
 }
@@ -809,11 +827,50 @@ CUresult logdet_run(CULAPACKhandle h, const T* x, long long incx, long long n, O
 // ------------------------------------------------------------------------------
 // Handle
 // ------------------------------------------------------------------------------
+namespace {
+
+// Releases whatever a handle holds (any member may still be null).
+void release_handle(CULAPACKhandle h) {
+  if (h->s_panel != nullptr) cudaStreamSynchronize(h->s_panel);
+  if (h->s_update != nullptr) cudaStreamSynchronize(h->s_update);
+  cudaFree(h->ws);
+  cudaFree(h->d_words);
+  cudaFreeHost(h->h_words);
+  cudaFree(h->d_logdet);
+  cudaFree(h->d_logdet_f);
+  cudaFreeHost(h->h_logdet);
+  cudaFree(h->d_part);
+  cudaFree(h->d_counter);
+  cudaFree(h->desc_dev);
+  cudaFreeHost(h->desc_host);
+  if (h->ev_panel != nullptr) cudaEventDestroy(h->ev_panel);
+  if (h->ev_update != nullptr) cudaEventDestroy(h->ev_update);
+  if (h->s_panel != nullptr) cudaStreamDestroy(h->s_panel);
+  if (h->s_update != nullptr) cudaStreamDestroy(h->s_update);
+  delete h;
+}
+
+CUresult create_handle(CULAPACKhandle h);
+
+}  // namespace
+
 extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   if (handle == nullptr) return CUDA_ERROR_INVALID_VALUE;
   auto* h = new (std::nothrow) __culapackhandle_st;
   if (h == nullptr) return CUDA_ERROR_OUT_OF_MEMORY;
   memset(h, 0, sizeof(*h));
+  const CUresult rc = create_handle(h);
+  if (rc != CUDA_SUCCESS) {
+    release_handle(h);   // nothing of a failed creation is left behind
+    return rc;
+  }
+  *handle = h;
+  return CUDA_SUCCESS;
+}
+
+namespace {
+CUresult create_handle(CULAPACKhandle h) {
+  h->wait_limit = -1;
   CUCHOL_CHECK(cudaGetDevice(&h->device));
   {
     const char* e = getenv("CUCHOLESKY_FORCE_SIMT");   // testing: FP64 products on the SIMT engine
@@ -842,42 +899,40 @@ extern "C" CUCHOL_EXPORT CUresult cuLAPACKCreate(CULAPACKhandle* handle) {
   CUCHOL_CHECK(cudaStreamCreateWithPriority(&h->s_update, cudaStreamDefault, mid));
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_panel, cudaEventDisableTiming));
   CUCHOL_CHECK(cudaEventCreateWithFlags(&h->ev_update, cudaEventDisableTiming));
-  CUCHOL_CHECK(cudaMalloc(&h->d_words, 16 * sizeof(int)));
+  CUCHOL_CHECK(dev_malloc(&h->d_words, 16 * sizeof(int)));
   CUCHOL_CHECK(cudaMemset(h->d_words, 0, 16 * sizeof(int)));
   CUCHOL_CHECK(cudaMallocHost(&h->h_words, 16 * sizeof(int)));
-  CUCHOL_CHECK(cudaMalloc(&h->d_logdet, 4 * sizeof(double)));
-  CUCHOL_CHECK(cudaMalloc(&h->d_logdet_f, 4 * sizeof(float)));
+  CUCHOL_CHECK(dev_malloc(&h->d_logdet, 4 * sizeof(double)));
+  CUCHOL_CHECK(dev_malloc(&h->d_logdet_f, 4 * sizeof(float)));
   CUCHOL_CHECK(cudaMallocHost(&h->h_logdet, 4 * sizeof(double)));
-  CUCHOL_CHECK(cudaMalloc(&h->d_part, kLogdetMaxBlocks * sizeof(double)));
-  CUCHOL_CHECK(cudaMalloc(&h->d_counter, sizeof(unsigned int)));
+  CUCHOL_CHECK(dev_malloc(&h->d_part, kLogdetMaxBlocks * sizeof(double)));
+  CUCHOL_CHECK(dev_malloc(&h->d_counter, sizeof(unsigned int)));
   CUCHOL_CHECK(cudaMemset(h->d_counter, 0, sizeof(unsigned int)));
   h->desc_bytes = size_t(8) << 20;
-  CUCHOL_CHECK(cudaMalloc(&h->desc_dev, h->desc_bytes));
+  CUCHOL_CHECK(dev_malloc(&h->desc_dev, h->desc_bytes));
   CUCHOL_CHECK(cudaMallocHost(&h->desc_host, h->desc_bytes));
   CUCHOL_CHECK(cudaDeviceSynchronize());
-  *handle = h;
   return CUDA_SUCCESS;
 }
+}  // namespace
 
 extern "C" CUCHOL_EXPORT CUresult cuLAPACKDestroy(CULAPACKhandle h) {
   if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
   CUCHOL_CHECK(cudaStreamSynchronize(h->s_panel));
   CUCHOL_CHECK(cudaStreamSynchronize(h->s_update));
-  cudaFree(h->ws);
-  cudaFree(h->d_words);
-  cudaFreeHost(h->h_words);
-  cudaFree(h->d_logdet);
-  cudaFree(h->d_logdet_f);
-  cudaFreeHost(h->h_logdet);
-  cudaFree(h->d_part);
-  cudaFree(h->d_counter);
-  cudaFree(h->desc_dev);
-  cudaFreeHost(h->desc_host);
-  cudaEventDestroy(h->ev_panel);
-  cudaEventDestroy(h->ev_update);
-  cudaStreamDestroy(h->s_panel);
-  cudaStreamDestroy(h->s_update);
-  delete h;
+  release_handle(h);
+  return CUDA_SUCCESS;
+}
+
+// ---- testing hooks (include/cucholesky_ext.h) ---------------------------------------
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKFailAllocation(int after) {
+  g_fail_after.store(after < 0 ? -1 : after);
+  return CUDA_SUCCESS;
+}
+
+extern "C" CUCHOL_EXPORT CUresult cuLAPACKSetWaitLimit(CULAPACKhandle h, int iterations) {
+  if (h == nullptr) return CUDA_ERROR_INVALID_VALUE;
+  h->wait_limit = iterations;
   return CUDA_SUCCESS;
 }
 

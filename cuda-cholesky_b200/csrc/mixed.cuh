@@ -145,10 +145,12 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Thread 0 waits until *ready >= need (bounded); returns the value seen.  A wait
-// that gives up sets *err and returns `need`, so that the solve still ends.
-__device__ __forceinline__ unsigned wait_ready(const unsigned* ready, unsigned need, int* err) {
-  for (unsigned it = 0; it < (1u << 24); ++it) {
+// Thread 0 waits until *ready >= need, for at most `limit` polls (limit < 0: 2^24,
+// seconds); returns the value seen.  A wait that gives up sets *err and returns
+// `need`, so that the solve still ends (with a wrong result the host then discards).
+__device__ __forceinline__ unsigned wait_ready(const unsigned* ready, unsigned need, int* err, int limit) {
+  const unsigned polls = limit < 0 ? (1u << 24) : (unsigned)limit;
+  for (unsigned it = 0; it < polls; ++it) {
     const unsigned v = ld_acquire(ready);
     if (v >= need) return v;
     if (it > 64) __nanosleep(64);
@@ -167,7 +169,7 @@ template <typename T, typename VB>
 __global__ void __launch_bounds__(kThreads)
     trsv_fwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
                     const VB* __restrict__ B, long long ldb, const double* __restrict__ sc, T* Y, long long ldy,
-                    int nrhs, unsigned* ctr, int* err) {
+                    int nrhs, unsigned* ctr, int* err, int wait_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto Ls = reinterpret_cast<T(*)[BS + 1]>(smem_raw);           // [BS][BS + 1]
   auto Ds = reinterpret_cast<T(*)[BS + 1]>(smem_raw + sizeof(T) * BS * (BS + 1));
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kThreads)
       Ls[ii][jj] = pre[q];
     }
     if (J + 1 < I) fetch(J + 1);
-    if (t == 0 && s_known < (unsigned)(J + 1)) s_known = wait_ready(&ctr[1], (unsigned)(J + 1), err);
+    if (t == 0 && s_known < (unsigned)(J + 1)) s_known = wait_ready(&ctr[1], (unsigned)(J + 1), err, wait_limit);
     __syncthreads();
     {
       const int jj = t >> 4, c = t & 15;   // y_J into shared memory (L2 reads: written by another CTA)
@@ -259,7 +261,7 @@ template <typename T, typename VZ>
 __global__ void __launch_bounds__(kThreads)
     trsv_bwd_kernel(const T* __restrict__ L, long long rs, long long cs, int n, const T* __restrict__ DI,
                     const T* Y, long long ldy, const double* __restrict__ sc, VZ* Z, long long ldz, T* Zt,
-                    int nrhs, unsigned* ctr, int* err) {
+                    int nrhs, unsigned* ctr, int* err, int wait_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto Ls = reinterpret_cast<T(*)[BS + 1]>(smem_raw);           // Ls[c][r] = L(J*BS + c, I*BS + r)
   auto Ds = reinterpret_cast<T(*)[BS + 1]>(smem_raw + sizeof(T) * BS * (BS + 1));   // Ds[r][c] = DI_I(c, r)
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (J - 1 > I) fetch(J - 1);
     const unsigned need = (unsigned)(nblk - J);
-    if (t == 0 && s_known < need) s_known = wait_ready(&ctr[1], need, err);
+    if (t == 0 && s_known < need) s_known = wait_ready(&ctr[1], need, err, wait_limit);
     __syncthreads();
     {
       const int jj = t >> 4, c = t & 15;
@@ -1360,34 +1362,34 @@ CUresult mixed_create(CUcholMixed* out, CULAPACKhandle h, CBlasUplo uplo, size_t
     return ::cuchol::report(e, "cudaMalloc", __func__, __FILE__, __LINE__);
   };
   cudaError_t e;
-  if ((e = cudaMalloc(&p->W, sizeof(float) * p->ldw * n)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->s, sizeof(double) * n)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->W, sizeof(float) * p->ldw * n)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->s, sizeof(double) * n)) != cudaSuccess) return fail(e);
   const int nT = (n + NBT - 1) / NBT;
-  if ((e = cudaMalloc(&p->Dinv, sizeof(float) * (size_t)nT * NBT * NBT)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->dtmp, sizeof(float) * (size_t)n * NBT / 4 + 256)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->Dinv, sizeof(float) * (size_t)nT * NBT * NBT)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->dtmp, sizeof(float) * (size_t)n * NBT / 4 + 256)) != cudaSuccess) return fail(e);
   // split k only when a GEMV has fewer than 2 * SMs row blocks: at most NBT / 256 splits
   const size_t gpart = (size_t)(NBT / 256) * (2 * h->num_sms + 1) * GR * NR;
-  if ((e = cudaMalloc(&p->gpart, sizeof(float) * gpart)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->gpart, sizeof(float) * gpart)) != cudaSuccess) return fail(e);
   // x r z p q b in one block, then the reduction scratch
-  if ((e = cudaMalloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->x, sizeof(double) * 6 * p->ld * NR)) != cudaSuccess) return fail(e);
   p->r = p->x + p->ld * NR;
   p->z = p->r + p->ld * NR;
   p->p = p->z + p->ld * NR;
   p->q = p->p + p->ld * NR;
   p->b = p->q + p->ld * NR;
-  if ((e = cudaMalloc(&p->t, sizeof(float) * 3 * p->ld * NR)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->t, sizeof(float) * 3 * p->ld * NR)) != cudaSuccess) return fail(e);
   p->y = p->t + p->ld * NR;
   p->zf = p->y + p->ld * NR;
   const size_t ptile = (size_t)T * (T + 1) / 2 * SY * NR;
-  if ((e = cudaMalloc(&p->U, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->V, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&p->part, sizeof(double) * (kVecBlocks * NR + kVecBlocks * 2 * NR + 2 * NR + 2 * NR))) !=
+  if ((e = dev_malloc(&p->U, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->V, sizeof(double) * ptile)) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->part, sizeof(double) * (kVecBlocks * NR + kVecBlocks * 2 * NR + 2 * NR + 2 * NR))) !=
       cudaSuccess)
     return fail(e);
   p->part_norm = p->part + kVecBlocks * NR;
   p->rz = p->part_norm + kVecBlocks * 2 * NR;
   p->norms = p->rz + 2 * NR;
-  if ((e = cudaMalloc(&p->ctr, 16 * sizeof(unsigned))) != cudaSuccess) return fail(e);
+  if ((e = dev_malloc(&p->ctr, 16 * sizeof(unsigned))) != cudaSuccess) return fail(e);
   p->err = reinterpret_cast<int*>(p->ctr + 8);
   if ((e = cudaMemset(p->ctr, 0, 16 * sizeof(unsigned))) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&p->h_norms, 2 * NR * sizeof(double))) != cudaSuccess) return fail(e);
@@ -1502,10 +1504,11 @@ CUresult potrs_run(CULAPACKhandle h, bool upper, int n, int nrhs, const T* A, lo
     const int nc = std::min(NR, nrhs - g0);
     T* Bg = B + (long long)g0 * ldb;
     CUCHOL_CHECK(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned), s));
-    trsv_fwd_kernel<T, T><<<nblk, kThreads, trsv_smem<T>(), s>>>(A, rs, cs, n, DI, Bg, ldb, nullptr, Y, ldy, nc, ctr, err);
+    trsv_fwd_kernel<T, T><<<nblk, kThreads, trsv_smem<T>(), s>>>(A, rs, cs, n, DI, Bg, ldb, nullptr, Y, ldy, nc, ctr, err,
+                                                                      h->wait_limit);
     CUCHOL_CHECK(cudaGetLastError());
     trsv_bwd_kernel<T, T><<<nblk, kThreads, trsv_smem<T>(), s>>>(A, rs, cs, n, DI, Y, ldy, nullptr, Bg, ldb, Y, nc, ctr + 2,
-                                                    err);
+                                                    err, h->wait_limit);
     CUCHOL_CHECK(cudaGetLastError());
     h->launches += 2;
   }

@@ -88,7 +88,7 @@ def extension_symbols() -> list[str]:
               "cuDpotrs", "cuSpotrs", "cuDcholMixedCreate", "cuDcholMixedRefactor", "cuDcholMixedSolve",
               "cuCholMixedGetFactor", "cuSsyrkLowp", "cuDpotrfOzaki",
               "cuCholMixedDestroy", "cuDposvMixed", "cuMultiGPULAPACKGetStats", "cuSlatmc", "cuDlatmc", "cuClatmc",
-              "cuZlatmc", "philox32_t", "philox64_t"]
+              "cuZlatmc", "philox32_t", "philox64_t", "cuLAPACKFailAllocation", "cuLAPACKSetWaitLimit"]
     for b in ("32", "64"):
         names += [f"cuRng{b}{f}" for f in ("Create", "Destroy", "Set", "Get", "GetOpenOpen", "GetOpenClose",
                                            "GetCloseOpen", "GetCloseClose")]

@@ -96,6 +96,25 @@ CUresult cuCholBatchedDestroy(CUcholBatched);
 CUresult cuDlogdetNoAlloc(CUdeviceptr x, size_t incx, size_t n, double *result, CUstream stream);
 
 
+/* Testing hooks for the failure paths (no counterpart in the reference library,
+ * whose failure reporting is the CUresult of each call plus the errorHandler
+ * callback, include/error.h:42-65 and multigpu/error.c:4-11).  Neither is needed in
+ * normal use.
+ *   cuLAPACKFailAllocation   after `after` more device allocations by this library
+ *                            have succeeded, the next one fails as if the device
+ *                            were out of memory (no cudaMalloc is attempted for it),
+ *                            once: the routine that asked returns
+ *                            CUDA_ERROR_OUT_OF_MEMORY through errorHandler, frees
+ *                            what it had allocated, and its handle stays usable.
+ *                            after < 0 clears a pending failure.
+ *   cuLAPACKSetWaitLimit     the ticket-ordered triangular solves of cu?potrs poll a
+ *                            counter that earlier blocks raise; a wait gives up after
+ *                            `iterations` polls (< 0: the default, seconds), and the
+ *                            call then returns CUDA_ERROR_LAUNCH_TIMEOUT through
+ *                            errorHandler.  0 makes every such wait give up at once. */
+CUresult cuLAPACKFailAllocation(int after);
+CUresult cuLAPACKSetWaitLimit(CULAPACKhandle, int iterations);
+
 /* ?POTRS: B := A^-1 B for the n x nrhs matrix B, from the Cholesky factor that
  * cu?potrf left in A (same uplo).  LAPACK DPOTRS semantics; the reference library
  * has no ?potrs (its SPD path stops at lapack/dpotrf.c:172 and dpotri.c:25).
