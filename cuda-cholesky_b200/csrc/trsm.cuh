@@ -108,28 +108,47 @@ __global__ void __launch_bounds__(256, sizeof(T) == 16 ? 1 : 2)
       }
     }
   }
-  if (row < m) {
+  // the solved 64-row tile, staged in shared memory (the L / X buffers are idle now),
+  // goes to each output in the order that is contiguous in that output
+  __syncthreads();
+  T* Xt = reinterpret_cast<T*>(smem_raw);   // [64][129]: Xt[r * 129 + col]
 #pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const int col = cg * 32 + k;
-      if (col < jb) {
-        B[(long long)row * brs + (long long)col * bcs] = cvt<TB>(x[k]);
-        const long long o = (long long)row * o_rs + (long long)col * o_cs;
-        if constexpr (MODE == OUT_ROUND) {
-          out2[o] = to_op<O2>((float)x[k]);
-        } else if constexpr (MODE == OUT_SPLIT) {
-          const float hi = round_tf32((float)x[k]);
-          out2[o] = hi;
-          out3[o] = round_tf32((float)x[k] - hi);
-        } else {
-          out2[o] = cvt<O2>(x[k]);
-        }
+  for (int k = 0; k < 32; ++k) Xt[r * 129 + cg * 32 + k] = x[k];
+  __syncthreads();
+  const int rows = min(64, m - (int)blockIdx.x * 64);
+  const long long row0 = (long long)blockIdx.x * 64;
+  auto put = [&](auto* out, long long rs_, long long cs_, auto conv) {
+    if (rs_ == 1) {        // rows contiguous: consecutive threads take consecutive rows
+      for (int e = t; e < 64 * jb; e += 256) {
+        const int rr = e & 63, c = e >> 6;
+        if (rr < rows) out[(row0 + rr) * rs_ + (long long)c * cs_] = conv(Xt[rr * 129 + c]);
+      }
+    } else {               // columns contiguous (or neither): consecutive threads take consecutive columns
+      for (int e = t; e < rows * jb; e += 256) {
+        const int rr = e / jb, c = e - rr * jb;
+        out[(row0 + rr) * rs_ + (long long)c * cs_] = conv(Xt[rr * 129 + c]);
       }
     }
+  };
+  put(B, brs, bcs, [](T v) { return cvt<TB>(v); });
+  if constexpr (MODE == OUT_ROUND) {
+    put(out2, o_rs, o_cs, [](T v) { return to_op<O2>((float)v); });
+  } else if constexpr (MODE == OUT_SPLIT) {
+    put(out2, o_rs, o_cs, [](T v) { return round_tf32((float)v); });
+    put(out3, o_rs, o_cs, [](T v) {
+      const float hi = round_tf32((float)v);
+      return round_tf32((float)v - hi);
+    });
+  } else {
+    put(out2, o_rs, o_cs, [](T v) { return cvt<O2>(v); });
   }
 }
 
+// Shared memory of trsm_rows_kernel: the diagonal block rows, the published solved
+// block and the reciprocal pivots, and later the 64 x 128 output tile (padded).
 template <typename T>
-constexpr size_t trsm_rows_smem() { return sizeof(T) * (128 * 33 + 64 * 33 + 32); }
+constexpr size_t trsm_rows_smem() {
+  return sizeof(T) * ((128 * 33 + 64 * 33 + 32) > 64 * 129 ? (128 * 33 + 64 * 33 + 32) : 64 * 129);
+}
 
 }  // namespace cuchol
