@@ -30,7 +30,7 @@ template <typename T>
 __global__ void copy_view_kernel(const T* __restrict__ src, long long s_rs, long long s_cs,
                                  T* __restrict__ dst, long long d_rs, long long d_cs,
                                  int m, int n, int lower_only, const int* __restrict__ abort_flag) {
-  if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
+  if (cta_aborted(abort_flag)) return;
   // 32 x 8 tiles; the faster index follows the unit stride of the destination
   const bool rows_fast = (d_rs == 1);
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;

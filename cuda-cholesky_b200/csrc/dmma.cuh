@@ -40,7 +40,8 @@ constexpr int A_STAGE = BM * BK * 8;               // 16 KB
 constexpr int B_STAGE = BN * BK * 8;               // 8 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
-constexpr unsigned kSpinLimit = 1u << 26;          // bounded mbarrier waits (~seconds)
+constexpr unsigned kSpinLimit = 1u << 26;          // bounded mbarrier waits: at most 2^26 polls
+constexpr unsigned long long kWaitNs = 1000000000ull;   // and at most one second
 
 enum : int { LAYOUT_R = 0, LAYOUT_K = 1 };
 
@@ -78,10 +79,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: false if it gave up
+// bounded wait (polls and wall-clock time; a poll may suspend the thread for a while):
+// false if it gave up
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (unsigned it = 0; it < kSpinLimit; ++it)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 15u) == 15u && global_ns() - t0 > kWaitNs) return false;
+  }
   return false;
 }
 __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y) {
@@ -122,7 +128,7 @@ template <int LA, int LB, bool TRI>
 __global__ void __launch_bounds__(THREADS, 2)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
-  if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
+  if (cta_aborted(abort_flag)) return;
   // This CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...  The host picks the
   // grid so that a CTA handles several tiles: the TMA ring keeps streaming across
   // tile boundaries, while CTAs still retire often enough for other streams' kernels.

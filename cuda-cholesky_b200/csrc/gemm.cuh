@@ -86,10 +86,8 @@ __global__ void __launch_bounds__(256)
 gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict__ abort_flag) {
   constexpr int BM = 16 * TM, BN = 16 * TM, BK = SimtCfg<T>::BK, NT = 256;
   constexpr int LDA_PER = BM * BK / NT, LDB_PER = BN * BK / NT;
-  if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
-
   const GemmProblem<T>& P = *find_problem(L, blockIdx.x);
-  if (P.stop != nullptr && *(volatile const int*)P.stop != 0) return;
+  if (cta_aborted(abort_flag, P.stop)) return;
   const int tile = blockIdx.x - P.tile_begin;
   const int ti = tile / P.tiles_n, tj = tile % P.tiles_n;
   const int i0 = ti * BM, j0 = tj * BN;
@@ -196,6 +194,142 @@ gemm_simt_kernel(const __grid_constant__ GemmLaunch<T> L, const int* __restrict_
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 tensor-core form of the grouped engine: the same problems, tiles (64 x 64,
+// numbered as by gemm_simt_kernel) and masked, coalesced global loads (register
+// staged, double-buffered shared memory), with the products on the warp-level DMMA
+// instruction (mma.sync m16n8k4 f64): four warps of 32 x 32 outputs (2 m16 x 4 n8
+// blocks).  Shared rows hold one k of 64 rows, padded to 68 doubles, so that the
+// 16 lanes of each half warp (rows g = 0..3 or 4..7, k slots t = 0..3) read 16
+// distinct bank pairs: 2g + 8t mod 32.  Used for FP64 problems that the TMA-fed
+// engine does not take: grouped launches (problem lists of many small products,
+// the batched plans and the recursive ?trtri levels) and unaligned views.
+// ---------------------------------------------------------------------------------
+constexpr int kDgBM = 64, kDgBK = 16, kDgThreads = 128, kDgLD = kDgBM + 4;
+
+__device__ __forceinline__ void dmma_m16n8k4(double (&d)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(kDgThreads)
+gemm_dmma_group_kernel(const __grid_constant__ GemmLaunch<double> L, const int* __restrict__ abort_flag) {
+  constexpr int BM = kDgBM, BN = kDgBM, BK = kDgBK, NT = kDgThreads, LDS = kDgLD;
+  constexpr int PER = BM * BK / NT;   // elements of each operand a thread loads per k block
+  const GemmProblem<double>& P = *find_problem(L, blockIdx.x);
+  if (cta_aborted(abort_flag, P.stop)) return;
+  const int tile = blockIdx.x - P.tile_begin;
+  const int ti = tile / P.tiles_n, tj = tile % P.tiles_n;
+  const int i0 = ti * BM, j0 = tj * BN;
+  if (P.lower_only && j0 > i0 + BM - 1) return;
+  int kb, ke;
+  tile_k_range(P, i0, j0, BM, BN, kb, ke);
+
+  __shared__ __align__(16) double As[2][BK][LDS];
+  __shared__ __align__(16) double Bs[2][BK][LDS];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp & 1, wn = warp >> 1;   // warp rows wm*32 .., columns wn*32 ..
+  double acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+
+  double ra[PER], rb[PER];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * NT;
+      const int r = (LA == 0) ? e % BM : e / BK;
+      const int kk = (LA == 0) ? e / BM : e % BK;
+      const int i = i0 + r, k = k0 + kk;
+      double v = 0.0;
+      if (i < P.m && k < ke && k >= kb && tri_keep(P.tri_a, i, k)) v = (P.unit_a && i == k) ? 1.0 : P.a[i * P.a_rs + k * P.a_ks];
+      ra[q] = v;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * NT;
+      const int r = (LB == 0) ? e % BN : e / BK;
+      const int kk = (LB == 0) ? e / BN : e % BK;
+      const int j = j0 + r, k = k0 + kk;
+      double v = 0.0;
+      if (j < P.n && k < ke && k >= kb && tri_keep(P.tri_b, j, k)) v = (P.unit_b && j == k) ? 1.0 : P.b[j * P.b_rs + k * P.b_ks];
+      rb[q] = v;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * NT;
+      const int r = (LA == 0) ? e % BM : e / BK;
+      const int kk = (LA == 0) ? e / BM : e % BK;
+      As[buf][kk][r] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = tid + q * NT;
+      const int r = (LB == 0) ? e % BN : e / BK;
+      const int kk = (LB == 0) ? e / BN : e % BK;
+      Bs[buf][kk][r] = rb[q];
+    }
+  };
+
+  int k0 = (kb / BK) * BK;
+  if (k0 < ke) {
+    load(k0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (; k0 < ke; k0 += BK) {
+      const bool more = (k0 + BK < ke);
+      if (more) load(k0 + BK);
+#pragma unroll
+      for (int k4 = 0; k4 < BK; k4 += 4) {
+        const int kk = k4 + t;
+        double a0[2], a1[2], bv[4];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          a0[mb] = As[buf][kk][wm * 32 + mb * 16 + g];
+          a1[mb] = As[buf][kk][wm * 32 + mb * 16 + g + 8];
+        }
+#pragma unroll
+        for (int nb8 = 0; nb8 < 4; ++nb8) bv[nb8] = Bs[buf][kk][wn * 32 + nb8 * 8 + g];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+          for (int nb8 = 0; nb8 < 4; ++nb8) dmma_m16n8k4(acc[mb][nb8], a0[mb], a1[mb], bv[nb8]);
+      }
+      if (more) {
+        store(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+      }
+    }
+  }
+
+#pragma unroll
+  for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+    for (int nb8 = 0; nb8 < 4; ++nb8)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = i0 + wm * 32 + mb * 16 + g + (e >> 1) * 8;
+        const int j = j0 + wn * 32 + nb8 * 8 + 2 * t + (e & 1);
+        if (i < P.m && j < P.n && (!P.lower_only || i >= j)) {
+          double v = P.alpha * acc[mb][nb8][e];
+          if (P.cin != nullptr) v = fma(P.beta, P.cin[i * P.cin_rs + j * P.cin_cs], v);
+          P.c[i * P.c_rs + j * P.c_cs] = v;
+        }
+      }
 }
 
 }  // namespace cuchol

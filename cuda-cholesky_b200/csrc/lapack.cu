@@ -118,9 +118,27 @@ CUresult launch_simt(CULAPACKhandle h, const GemmLaunch<T>& L, int tiles, cudaSt
   return CUDA_SUCCESS;
 }
 
+template <int LA, int LB>
+CUresult launch_dmma_group(CULAPACKhandle h, const GemmLaunch<double>& L, int tiles, cudaStream_t s,
+                           const int* abort) {
+  gemm_dmma_group_kernel<LA, LB><<<tiles, kDgThreads, 0, s>>>(L, abort);
+  ++h->launches;
+  CUCHOL_CHECK(cudaGetLastError());
+  return CUDA_SUCCESS;
+}
+
 template <typename T, int TM = 4>
 CUresult launch_dispatch(CULAPACKhandle h, const GemmLaunch<T>& L, int tiles, int la, int lb, cudaStream_t s,
                          const int* abort) {
+  if constexpr (std::is_same<T, double>::value && TM == 4) {
+    // FP64 on the tensor cores (64 x 64 tiles, numbered as by the SIMT engine)
+    if (!h->force_simt) {
+      if (la == 0 && lb == 0) return launch_dmma_group<0, 0>(h, L, tiles, s, abort);
+      if (la == 0 && lb == 1) return launch_dmma_group<0, 1>(h, L, tiles, s, abort);
+      if (la == 1 && lb == 0) return launch_dmma_group<1, 0>(h, L, tiles, s, abort);
+      return launch_dmma_group<1, 1>(h, L, tiles, s, abort);
+    }
+  }
   if (la == 0 && lb == 0) return launch_simt<T, 0, 0, TM>(h, L, tiles, s, abort);
   if (la == 0 && lb == 1) return launch_simt<T, 0, 1, TM>(h, L, tiles, s, abort);
   if (la == 1 && lb == 0) return launch_simt<T, 1, 0, TM>(h, L, tiles, s, abort);

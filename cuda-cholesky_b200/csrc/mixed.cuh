@@ -86,7 +86,7 @@ __global__ void build_kernel(const double* __restrict__ a, long long rs, long lo
 // FP32 diagonal block of W -> FP64 copy D (ld SB); column j = blockIdx.x.
 __global__ void diag_in_kernel(const float* __restrict__ W, long long ldw, int jb, double* __restrict__ D,
                                const int* __restrict__ stop) {
-  if (*stop != 0) return;
+  if (cta_aborted(stop)) return;
   const int j = blockIdx.x, i = threadIdx.x;
   if (i < jb && i >= j) D[i + j * SB] = (double)W[i + (long long)j * ldw];
 }
@@ -94,7 +94,7 @@ __global__ void diag_in_kernel(const float* __restrict__ W, long long ldw, int j
 // Factored FP64 block -> W (FP32).
 __global__ void diag_out_kernel(const double* __restrict__ D, int jb, float* __restrict__ W, long long ldw,
                                 const int* __restrict__ stop) {
-  if (*stop != 0) return;
+  if (cta_aborted(stop)) return;
   const int j = blockIdx.x, i = threadIdx.x;
   if (i < jb && i >= j) W[i + (long long)j * ldw] = (float)D[i + j * SB];
 }

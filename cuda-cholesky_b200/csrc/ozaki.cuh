@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   __shared__ int s_fail, s_mma_a, s_mma_b;
   __shared__ double s_pc[BN];   // 2^e of the tile's columns
 
-  if (stop != nullptr && *stop != 0) return;
+  if (cta_aborted(stop)) return;
   int ti, tj;
   if (!tile_of(blockIdx.x, p, ti, tj)) return;
   const int row0 = ti * BM, col0 = tj * BN;
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256)
     slice_kernel(const double* __restrict__ P, long long prs, long long pcs, int R, int k, int S, int8_t* sl,
                  long long kp, int* __restrict__ expo, const int* stop) {
   __shared__ int s_e[8][32];
-  if (stop != nullptr && *stop != 0) return;
+  if (cta_aborted(stop)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r = blockIdx.x * 32 + lane;
   const int nseg = (int)(kp / 16);

@@ -324,7 +324,7 @@ __device__ __forceinline__ void diag_factor_block(T* __restrict__ A, long long r
   using R = RealOf<T>;
   using L = DiagSmem<T, NB>;
   constexpr int LD = L::LD;
-  if (*(volatile int*)d_info != 0) return;   // an earlier block already failed
+  if (cta_aborted(d_info)) return;   // an earlier block already failed
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S = reinterpret_cast<T*>(smem_raw);
   T* X = reinterpret_cast<T*>(smem_raw + L::S);
@@ -443,7 +443,7 @@ struct InvTask {
 template <typename T, int NB, int NT>
 __global__ void __launch_bounds__(NT) diag_invert_batched_kernel(const InvTask<T>* __restrict__ tasks) {
   const InvTask<T> t = tasks[blockIdx.x];
-  if (t.stop != nullptr && *(volatile const int*)t.stop != 0) return;
+  if (cta_aborted(t.stop)) return;
   diag_invert_block<T, NB, NT>(t.b, t.rs, t.cs, t.jb, t.unit);
 }
 

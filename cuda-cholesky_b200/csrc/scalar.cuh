@@ -105,4 +105,25 @@ __device__ __forceinline__ cuDoubleComplex recip(cuDoubleComplex a) { return cuC
 
 template <typename T> __device__ __forceinline__ T conj_if(T x, bool c) { return c ? cj(x) : x; }
 
+// CTA-uniform test of up to two abort words (the device info word of a
+// factorization, a per-problem stop word).  Thread 0 reads them once and the CTA
+// decides together: a word that a kernel on another stream sets while this CTA is
+// starting must not split it into threads that run and threads that exit, which
+// would leave the running ones waiting for the exited ones.  Every thread of the CTA
+// must call it, before any other barrier.
+__device__ __forceinline__ bool cta_aborted(const int* a, const int* b = nullptr) {
+  __shared__ int s_abort_word;
+  if (threadIdx.x == 0)
+    s_abort_word = (a != nullptr && *(volatile const int*)a != 0) || (b != nullptr && *(volatile const int*)b != 0);
+  __syncthreads();
+  return s_abort_word != 0;
+}
+
+// Nanoseconds of the GPU's global timer (for waits bounded in time).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 }  // namespace cuchol

@@ -22,6 +22,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include "scalar.cuh"
 
 namespace cuchol {
 namespace tc {
@@ -33,7 +34,8 @@ constexpr int BM = 128, BN = 128, ROW_BYTES = 128, STAGES = 3, THREADS = 128;
 constexpr int A_STAGE = BM * ROW_BYTES, B_STAGE = BN * ROW_BYTES;   // 16 KB each
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;               // + alignment slack
-constexpr unsigned kSpinLimit = 1u << 26;
+constexpr unsigned kSpinLimit = 1u << 26;              // bounded mbarrier waits: at most 2^26 polls
+constexpr unsigned long long kWaitNs = 1000000000ull;   // and at most one second
 constexpr int TMEM_COLS = 128;
 
 // Operand element types: BF16 (kind::f16, K = 16 per MMA) and TF32 held in FP32
@@ -68,7 +70,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
+// bounded wait (polls and wall-clock time; a poll may suspend the thread for a while)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  unsigned long long t0 = 0;
   for (unsigned it = 0; it < kSpinLimit; ++it) {
     uint32_t ok;
     asm volatile(
@@ -77,6 +81,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (ok) return true;
+    if (it == 0) t0 = global_ns();
+    else if ((it & 15u) == 15u && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
 }
@@ -224,7 +230,7 @@ __global__ void __launch_bounds__(THREADS, SPLIT3 ? 1 : 2)
   __shared__ uint32_t tmem_slot;
   __shared__ int s_consumed, s_fail;
 
-  if (stop != nullptr && *stop != 0) return;   // an earlier step failed; uniform for the CTA
+  if (cta_aborted(stop)) return;   // an earlier step failed
   int ti, tj;
   tile_of(blockIdx.x, p, ti, tj);
   const int row0 = ti * BM, col0 = tj * BN;

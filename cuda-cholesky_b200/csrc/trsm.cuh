@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 16 ? 1 : 2)
   T* Ls = reinterpret_cast<T*>(smem_raw);   // [128][33]: conj L(32b + j, 32b + k)
   T* Xs = Ls + 128 * 33;                    // [64][33]: solved block
   T* rd = Xs + 64 * 33;                     // [32]: 1 / L(32b + j, 32b + j)
-  if (*stop != 0) return;
+  if (cta_aborted(stop)) return;
   const int t = threadIdx.x, r = t & 63, cg = t >> 6;
   const int row = blockIdx.x * 64 + r;
   T x[32];

@@ -104,7 +104,7 @@ template <int LA, int LB, bool TRI>
 __global__ void __launch_bounds__(THREADS, 2)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
-  if (abort_flag != nullptr && *(volatile const int*)abort_flag != 0) return;
+  if (cta_aborted(abort_flag)) return;
   const int ntiles = P.tiles_m * P.tiles_n;
   auto tile_range = [&](int tile, int& i0, int& j0, int& kbase, int& KT) -> bool {
     i0 = (tile / P.tiles_n) * BM;
