@@ -30,6 +30,10 @@ struct __cucholbatched_st {
   void* d_w;                 // inverses of the current step's diagonal blocks
   void* d_work;              // TRTRI X blocks, then L^H L (sum of n_b^2 elements)
   std::vector<void*> d_lists;
+  int persistent;            // FP64: the whole sequence is one persistent kernel (bpersist.cuh)
+  int* d_next;               // its work-queue head
+  double* d_wp;              // its per-CTA inverses of the diagonal blocks (wp_tiles per CTA)
+  int wp_tiles;
   bool dry;                  // recording pass 1: build and upload lists, launch nothing
   bool reuse;                // recording pass 2 (under capture): reuse the uploaded lists
   size_t cursor;
@@ -92,9 +96,15 @@ namespace {
 
 constexpr int kBatchedMaxNb = 64;   // a 64-wide SIMT tile holds a whole panel: in-place solve
 
+template <typename T>
+CUresult record_persistent(CUcholBatched p, const BatchedShape<T>& sh, cudaStream_t s);
+
 // Enqueue the whole batched sequence on stream s (used under stream capture).
 template <typename T>
 CUresult record_batched(CUcholBatched p, const BatchedShape<T>& sh, int nb, cudaStream_t s) {
+  if constexpr (std::is_same<T, double>::value) {
+    if (p->persistent) return record_persistent<T>(p, sh, s);
+  }
   CULAPACKhandle h = p->h;
   using Smem = DiagSmem<T, kBatchedMaxNb>;
   const int B = sh.batch;
@@ -290,7 +300,10 @@ __global__ void set_identity_kernel(T* a, const long long* __restrict__ off, con
 // (the kernels do the same work for any SPD input) and keep the fastest.
 template <typename T>
 CUresult tune_nb(CUcholBatched p, const BatchedShape<T>& sh, int* best_nb) {
-  const int candidates[] = {32, 64};
+  // candidates: the grouped graphs with nb = 32 and 64, and (FP64) the persistent
+  // kernel, written nb = -1 here
+  std::vector<int> candidates = {32, 64};
+  if (std::is_same<T, double>::value) candidates.push_back(-1);
   std::vector<long long> off(sh.batch);
   long long total = 0;
   for (int b = 0; b < sh.batch; ++b) { off[b] = total; total += (long long)sh.n[b] * sh.n[b]; }
@@ -327,7 +340,8 @@ CUresult tune_nb(CUcholBatched p, const BatchedShape<T>& sh, int* best_nb) {
   cudaEvent_t e0 = res.e0, e1 = res.e1;
   CUresult rc = CUDA_SUCCESS;
   for (int nb : candidates) {
-    rc = build_graph<T>(p, id, nb);
+    p->persistent = (nb < 0);
+    rc = build_graph<T>(p, id, nb < 0 ? kBatchedMaxNb : nb);
     if (rc != CUDA_SUCCESS) break;
     float ms_min = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
@@ -354,8 +368,12 @@ namespace {
 template <typename T>
 CUresult batched_create(CUcholBatched* out, CULAPACKhandle h, char type, CBlasUplo uplo, int batch,
                         const int* n, const CUdeviceptr* A, const int* lda, int flags, int nb) {
+  // nb: 0 = tuned, 8..64 (multiple of 8) = the grouped graph with that block size,
+  // -1 = the persistent kernel (FP64 only)
+  const bool nb_ok = (nb == -1 && std::is_same<T, double>::value) ||
+                     (nb >= 0 && nb <= kBatchedMaxNb && (nb == 0 || nb % 8 == 0));
   if (out == nullptr || h == nullptr || batch <= 0 || n == nullptr || A == nullptr || lda == nullptr ||
-      (uplo != CBlasLower && uplo != CBlasUpper) || nb < 0 || nb > kBatchedMaxNb || (nb != 0 && nb % 8 != 0))
+      (uplo != CBlasLower && uplo != CBlasUpper) || !nb_ok)
     return CUDA_ERROR_INVALID_VALUE;
   BatchedShape<T> sh;
   sh.upper = (uplo == CBlasUpper);
@@ -384,6 +402,10 @@ CUresult batched_create(CUcholBatched* out, CULAPACKhandle h, char type, CBlasUp
   p->d_work = nullptr;
   p->graph = nullptr;
   p->exec = nullptr;
+  p->persistent = 0;
+  p->d_next = nullptr;
+  p->d_wp = nullptr;
+  p->wp_tiles = 1;
   p->dry = false;
   p->reuse = false;
   p->cursor = 0;
@@ -391,6 +413,7 @@ CUresult batched_create(CUcholBatched* out, CULAPACKhandle h, char type, CBlasUp
   auto fail = [&](CUresult r) {
     free_plan_memory(p);
     cudaFree(p->d_info); cudaFree(p->d_logdet); cudaFree(p->d_w); cudaFree(p->d_work);
+    cudaFree(p->d_next); cudaFree(p->d_wp);
     delete p;
     return r;
   };
@@ -404,11 +427,20 @@ CUresult batched_create(CUcholBatched* out, CULAPACKhandle h, char type, CBlasUp
       dev_malloc(&p->d_w, sizeof(T) * (size_t)batch * kBatchedMaxNb * kBatchedMaxNb) != cudaSuccess ||
       dev_malloc(&p->d_work, sizeof(T) * std::max<size_t>(work, 1)) != cudaSuccess)
     return fail(report(cudaGetLastError(), "cudaMalloc", __func__, __FILE__, __LINE__));
+  int nmax = 1;
+  for (int b = 0; b < batch; ++b) nmax = std::max(nmax, n[b]);
+  p->wp_tiles = (nmax + kBatchedMaxNb - 1) / kBatchedMaxNb;
+  if (std::is_same<T, double>::value &&
+      (dev_malloc(&p->d_next, sizeof(int)) != cudaSuccess ||
+       dev_malloc(&p->d_wp, sizeof(double) * (size_t)h->num_sms * p->wp_tiles * kBatchedMaxNb * kBatchedMaxNb) !=
+           cudaSuccess))
+    return fail(report(cudaGetLastError(), "cudaMalloc", __func__, __FILE__, __LINE__));
   if (nb == 0) {
     rc = tune_nb<T>(p, sh, &nb);
     if (rc != CUDA_SUCCESS) return fail(rc);
   }
-  rc = build_graph<T>(p, sh, nb);
+  p->persistent = (nb < 0);
+  rc = build_graph<T>(p, sh, nb < 0 ? kBatchedMaxNb : nb);
   if (rc != CUDA_SUCCESS) return fail(rc);
   *out = p;
   return CUDA_SUCCESS;
@@ -449,7 +481,7 @@ extern "C" CUCHOL_EXPORT CUresult cuCholBatchedResults(CUcholBatched p, long* in
 
 extern "C" CUCHOL_EXPORT CUresult cuCholBatchedGetBlockSize(CUcholBatched p, int* nb) {
   if (p == nullptr || nb == nullptr) return CUDA_ERROR_INVALID_VALUE;
-  *nb = p->nb;
+  *nb = p->persistent ? -1 : p->nb;
   return CUDA_SUCCESS;
 }
 
@@ -461,6 +493,8 @@ extern "C" CUCHOL_EXPORT CUresult cuCholBatchedDestroy(CUcholBatched p) {
   cudaFree(p->d_logdet);
   cudaFree(p->d_w);
   cudaFree(p->d_work);
+  cudaFree(p->d_next);
+  cudaFree(p->d_wp);
   delete p;
   return CUDA_SUCCESS;
 }

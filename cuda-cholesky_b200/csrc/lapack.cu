@@ -1269,6 +1269,7 @@ CUCHOL_API_RANKK(cuZherk, cuDoubleComplex, true)
 
 #include "blas3.cuh"
 #include "batched.cuh"
+#include "bpersist.cuh"
 #include "mixed.cuh"
 #include "ozaki_driver.cuh"
 #include "hostmem.cuh"

@@ -39,14 +39,15 @@ def _run(handle, p, mats, uplo, nb, flags=7, bad=None):
     return plan, T, info, ld, res
 
 
-@pytest.mark.parametrize("p", ["d", "s"])
+# nb: 0 = the plan's tuner picks; 32 / 64 = the graph of grouped launches with that
+# block size; -1 = the persistent kernel (FP64: one launch, matrices from a queue)
+@pytest.mark.parametrize("p,nb", [("d", 0), ("d", 32), ("d", 64), ("d", -1), ("s", 0), ("s", 32), ("s", 64)])
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("nb", [0, 32, 64])
 def test_batched_factor_logdet_inverse(handle, p, uplo, nb):
-    sizes = [1, 7, 8, 31, 33, 64, 65, 100, 128, 129, 200, 257, 300, 17, 90]
+    sizes = [1, 7, 8, 31, 33, 64, 65, 100, 128, 129, 200, 257, 300, 17, 90, 512, 449]
     mats = _batch(p, sizes, seed=11)
     plan, T, info, ld, res = _run(handle, p, mats, uplo, nb)
-    assert plan.nb in (32, 64) and (nb == 0 or plan.nb == nb)
+    assert plan.nb in ((32, 64, -1) if p == "d" else (32, 64)) and (nb == 0 or plan.nb == nb)
     tri = np.tril if uplo == "L" else np.triu
     for A, inv, inf, l in zip(mats, res, info, ld):
         n = A.shape[0]
@@ -64,11 +65,12 @@ def test_batched_factor_logdet_inverse(handle, p, uplo, nb):
             assert matgen.inverse_residual(A, inv, uplo) <= 10, n
 
 
-def test_batched_failure_is_per_matrix(handle):
+@pytest.mark.parametrize("nb", [64, -1])
+def test_batched_failure_is_per_matrix(handle, nb):
     sizes = [50, 120, 200, 70]
     mats = _batch("d", sizes, seed=3)
     mats[2][150, 150] = -1.0            # matrix 2 fails at leading minor 151
-    plan, T, info, ld, res = _run(handle, "d", mats, "L", 64)
+    plan, T, info, ld, res = _run(handle, "d", mats, "L", nb)
     assert info == [0, 0, 151, 0]
     for b in (0, 1, 3):
         assert matgen.inverse_residual(mats[b], res[b], "L") <= 10
@@ -81,10 +83,11 @@ def test_batched_failure_is_per_matrix(handle):
     assert info2 == info and np.allclose(ld2, ld)
 
 
-def test_batched_factor_only(handle):
+@pytest.mark.parametrize("nb", [32, -1])
+def test_batched_factor_only(handle, nb):
     sizes = [40, 80, 160]
     mats = _batch("d", sizes, seed=5)
-    plan, T, info, ld, res = _run(handle, "d", mats, "L", 32, flags=cc.BATCHED_POTRF | cc.BATCHED_LOGDET)
+    plan, T, info, ld, res = _run(handle, "d", mats, "L", nb, flags=cc.BATCHED_POTRF | cc.BATCHED_LOGDET)
     for A, F, inf in zip(mats, res, info):
         assert inf == 0
         assert matgen.backward_error(A, F, "L") <= 10
