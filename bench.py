@@ -88,6 +88,12 @@ def parse():
                          "rank K (warm-up + measured), for profiling")
     ap.add_argument("--syrk-type", default="D", choices=["D", "Z"],
                     help="--syrk element type: D (cuDsyrk) or Z (cuZherk)")
+    ap.add_argument("--single", nargs=2, metavar=("P", "N"),
+                    help="only one cu<P>potrf of order N (P in S D C Z, --uplo), after one untimed call: "
+                         "for profiling")
+    ap.add_argument("--batch", type=int, default=10000, help="batched workload: number of matrices")
+    ap.add_argument("--batched-nb", type=int, default=0,
+                    help="batched workload: plan block size (0 tuned, 32 / 64 grouped graph, -1 persistent)")
     ap.add_argument("--syrk-lowp", nargs=3, metavar=("M", "K", "PREC"),
                     help="only the mixed factor's trailing update: two cuSsyrkLowp launches of order M, "
                          "rank K, PREC bf16 or tf32 (warm-up + measured), for profiling")
@@ -540,7 +546,7 @@ def batched_inputs(torch, dev, mine, sizes_all, tdt):
     return buf0, sizes, off
 
 
-def batched_result(torch, cc, p, warmup, steps, peak, rank=0, world=1, pg=None, dev=None):
+def batched_result(torch, cc, p, warmup, steps, peak, rank=0, world=1, pg=None, dev=None, batch=10000, nb=0):
     """10,000 squared-exponential kernel matrices K_ij = exp(-|x_i - x_j|^2 / (2 * 0.3^2))
     + 1e-4 delta_ij on n_i ~ U{8..512} points x ~ U[0,1]^3 (seed 0): factor, log det
     and inverse of every matrix in one graph launch of a batched plan, against looping
@@ -550,15 +556,15 @@ def batched_result(torch, cc, p, warmup, steps, peak, rank=0, world=1, pg=None, 
     from cucholesky import shard
     dev = dev if dev is not None else torch.device("cuda", 0)
     tdt = torch.float64 if p == "d" else torch.float32
-    B = 10000
+    B = batch
     rng = np.random.default_rng(0)
-    sizes_all = rng.integers(8, 513, B).tolist()
+    sizes_all = rng.integers(8, 513, 10000).tolist()[:B]   # the first B of the 10,000-matrix workload
     mine = shard.partition_by_cost(sizes_all, world)[rank] if world > 1 else list(range(B))
     buf0, sizes, off = batched_inputs(torch, dev, mine, sizes_all, tdt)
     buf = buf0.clone()
     h = cc.Handle()
     t0 = time.perf_counter()
-    plan = cc.BatchedPlan(h, buf, sizes, off, flags=7, nb=0)
+    plan = cc.BatchedPlan(h, buf, sizes, off, flags=7, nb=nb)
     plan_s = time.perf_counter() - t0
     flops = float(sum(n ** 3 for n in sizes_all))    # n^3/3 (potrf) + 2n^3/3 (potri), whole batch
     for _ in range(warmup):
@@ -634,7 +640,7 @@ def batched_result(torch, cc, p, warmup, steps, peak, rank=0, world=1, pg=None, 
     return {
         "metric": "batched_potrf_logdet_potri_matrices_per_s", "value": B / (ms / 1e3), "unit": "matrices/s",
         "dtype": "f64" if p == "d" else "f32", "ms_per_step": ms, "steps": steps, "warmup": warmup,
-        "workload": "10,000 squared-exponential kernel matrices, n_i ~ U{8..512}, lower",
+        "workload": f"{B:,} squared-exponential kernel matrices, n_i ~ U{{8..512}}, lower",
         "batch": B, "sum_n3": flops, "graph_launches_per_step": 1, "nb": nb,
         "gflops": gfl,
         "loop_of_plain_calls_ms_extrapolated": loop_total_ms,
@@ -760,6 +766,25 @@ def run_syrk_only(m: int, k: int, prefix: str = "D") -> None:
         print(json.dumps({"kernel": "cuDsyrk L,N" if prefix == "D" else "cuZherk L,N", "m": m, "k": k, "rc": rc,
                           "ms": ms, "tflops": mult * float(m) * (m + 1) * k / (ms / 1e3) / 1e12}), flush=True)
     bh.close()
+
+
+def run_single(prefix: str, n: int, uplo: str) -> None:
+    import torch
+    import cucholesky as cc
+    from cucholesky import matgen
+    p = prefix.lower()
+    h = cc.Handle()
+    A0 = matgen.spd_device(p, n, seed=1).to(matgen.torch_dtype(p))
+    A = torch.empty_like(A0)
+    for it in range(2):
+        A.copy_(A0)
+        ms, (rc, info) = timed(torch, lambda: cc.call_potrf(h, prefix.upper(), uplo, n, A.data_ptr(), n))
+        if rc != 0 or info != 0:
+            raise RuntimeError(f"cu{prefix}potrf rc={rc} info={info}")
+    mult = 4 if p in "cz" else 1
+    print(json.dumps({"routine": f"cu{prefix.upper()}potrf", "uplo": uplo, "n": n, "ms": ms,
+                      "tflops": mult * n ** 3 / 3 / (ms / 1e3) / 1e12}), flush=True)
+    h.close()
 
 
 def run_syrk_lowp_only(m: int, k: int, prec: str) -> None:
@@ -978,6 +1003,9 @@ def main():
     if args.syrk_lowp:
         run_syrk_lowp_only(int(args.syrk_lowp[0]), int(args.syrk_lowp[1]), args.syrk_lowp[2])
         return
+    if args.single:
+        run_single(args.single[0], int(args.single[1]), args.uplo)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return
@@ -1011,7 +1039,8 @@ def main():
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
             pg = dist
         peak, _ = fp64_peak_tflops(torch, dev, local)
-        r = batched_result(torch, cc, args.dtype, args.warmup, args.steps, peak, rank, world, pg, dev)
+        r = batched_result(torch, cc, args.dtype, args.warmup, args.steps, peak, rank, world, pg, dev,
+                           batch=args.batch, nb=args.batched_nb)
         if r is not None:
             r.update({"n_gpus": world, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
                       "vs_baseline": None, "data": "synthetic",
