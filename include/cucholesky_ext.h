@@ -45,13 +45,18 @@ CUresult cuLAPACKGetPotrfBlocks(CULAPACKhandle, char, size_t, int *);
  * (each matrix b: order n[b], device pointer A[b], leading dimension lda[b], all
  * in the same `uplo` storage).  No counterpart in the reference library.
  *
- * A plan records the whole sequence once into a CUDA graph: all matrices advance
- * one nb-wide block column per step, and each step is a few grouped launches over
- * the batch (diagonal blocks, panel solves, trailing updates), followed, with
- * CUCHOL_BATCHED_POTRI, by the grouped inverse.  nb = 0 lets the plan pick the
- * block size by timing the candidates (32, 64) on an identity batch of the same
- * shapes; otherwise nb must be 8..64 and a multiple of 8.  The plan keeps the
- * pointers: run it again after refilling the same buffers.
+ * A plan records its whole sequence once into a CUDA graph, in one of two forms:
+ *   nb = 8..64 (a multiple of 8): all matrices advance one nb-wide block column per
+ *     step, and each step is a few grouped launches over the batch (diagonal blocks,
+ *     panel solves, trailing updates), followed, with CUCHOL_BATCHED_POTRI, by the
+ *     grouped inverse;
+ *   nb = -1 (FP64 only): one persistent kernel; each CTA takes whole matrices from a
+ *     queue ordered by size, largest first, and factors, log-dets and inverts each in
+ *     place with 64 x 64 tile products on the FP64 tensor cores.
+ * nb = 0 lets the plan pick by timing the candidates (grouped with nb 32 and 64, and
+ * the persistent kernel for FP64) on an identity batch of the same shapes.  The plan
+ * keeps the pointers: run it again after refilling the same buffers.
+ * cuCholBatchedGetBlockSize reports the chosen nb (-1: the persistent kernel).
  *   cu?cholBatchedCreate  build (and tune) the plan; allocates its workspace
  *   cuCholBatchedRun      one graph launch on `stream`
  *   cuCholBatchedResults  waits, then copies info[b] (as ?potrf / ?potri) and
