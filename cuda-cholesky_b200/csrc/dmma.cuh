@@ -5,9 +5,13 @@
 // TFLOP/s device-wide, the same rate as DFMA).  Operand tiles are staged into
 // shared memory by TMA (cp.async.bulk.tensor.2d, 128-byte swizzle, no multicast)
 // through a 4-stage ring: thread 0 issues the copies (completion tracked by one
-// mbarrier per stage), and the CTA's four warps (2 x 2, 64 x 32 each) run the MMAs
-// on a 128 x 64 tile.  No dedicated producer warp: with 4 warps of at most 255
-// registers two CTAs fit on an SM, so 8 MMA warps hide each other's latency.
+// "full" mbarrier per stage), and the CTA's four warps (2 x 2) run the MMAs on a
+// 128 x 64 tile (warps of 64 x 32, two CTAs per SM) or a 64 x 64 tile (warps of
+// 32 x 32, three CTAs per SM).  No dedicated producer warp: it would not fit the
+// register budget of several CTAs per SM.  No CTA-wide barrier in the k loop either:
+// each warp releases a stage by arriving on its "empty" mbarrier, and thread 0, after
+// consuming item q, refills the stage of item q - 1 (which the other warps have almost
+// always released by then), so the warps drift freely within the ring.
 //
 // Problem form: the GemmProblem of gemm.cuh for T = double,
 //     C(i, j) = alpha * sum_k Ahat(i, k) * Bhat(j, k) + beta * Cin(i, j),
@@ -33,13 +37,22 @@
 namespace cuchol {
 namespace dmma {
 
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 4;
-constexpr int WARPS = 4;                           // 2 x 2 warps of 64 x 32
+constexpr int BN = 64, BK = 16;
+constexpr int WARPS = 4;                           // 2 x 2 warps of (16 MB) x 32
 constexpr int THREADS = WARPS * 32;
-constexpr int A_STAGE = BM * BK * 8;               // 16 KB
 constexpr int B_STAGE = BN * BK * 8;               // 8 KB
-constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
+
+// A tile shape: MB m16 blocks per warp, so BM = 32 MB rows per CTA (MB = 4: 128 x 64
+// tiles, two CTAs per SM; MB = 2: 64 x 64 tiles, fewer registers, three CTAs per SM).
+template <int MB>
+struct Shape {
+  static constexpr int BM = 32 * MB;
+  static constexpr int STAGES = 4;
+  static constexpr int MIN_CTAS = MB == 4 ? 2 : 3;  // CTAs per SM the registers allow
+  static constexpr int A_STAGE = BM * BK * 8;       // 16 KB (MB = 4) or 8 KB
+  static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
+};
 constexpr unsigned kSpinLimit = 1u << 26;          // bounded mbarrier waits: at most 2^26 polls
 constexpr unsigned long long kWaitNs = 1000000000ull;   // and at most one second
 
@@ -69,6 +82,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -124,10 +140,12 @@ __device__ __forceinline__ double tri_mask(double v, int tri, int unit, int row,
   return v;
 }
 
-template <int LA, int LB, bool TRI>
-__global__ void __launch_bounds__(THREADS, 2)
+template <int LA, int LB, bool TRI, int MB>
+__global__ void __launch_bounds__(THREADS, Shape<MB>::MIN_CTAS)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
+  constexpr int BM = Shape<MB>::BM, STAGES = Shape<MB>::STAGES;
+  constexpr int A_STAGE = Shape<MB>::A_STAGE, STAGE_BYTES = Shape<MB>::STAGE_BYTES;
   if (cta_aborted(abort_flag)) return;
   // This CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...  The host picks the
   // grid so that a CTA handles several tiles: the TMA ring keeps streaming across
@@ -153,10 +171,14 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&full_bar[s], 1);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], WARPS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -181,9 +203,20 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     ++issued;
     return true;
   };
+  bool more = true;   // thread 0: items are left to issue
   if (threadIdx.x == 0)
-    for (int q = 0; q < STAGES && produce(); ++q) {
+    for (int q = 0; q < STAGES && more; ++q) more = produce();
+  // thread 0, after consuming item `consumed`: issue the items up to consumed - 1 +
+  // STAGES, each into a stage whose previous item every warp has released (bounded
+  // wait); false if a wait gave up
+  auto refill = [&]() -> bool {
+    while (more && issued < consumed + STAGES) {
+      const long long old = issued - STAGES;
+      if (!mbar_wait(&empty_bar[old % STAGES], (unsigned)((old / STAGES) & 1))) return false;
+      more = produce();
     }
+    return true;
+  };
 
   // ---------------- MMA warps ----------------
   const int wm = warp & 1, wn = warp >> 1;
@@ -197,7 +230,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
   int i0, j0, kbase, KT;
   if (!tile_range(tile, i0, j0, kbase, KT)) continue;
-  double acc[4][4][4];
+  double acc[MB][4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -205,7 +238,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
 
-  const int wrow = i0 + wm * 64, wcol = j0 + wn * 32;   // first row / column of the warp
+  const int wrow = i0 + wm * (16 * MB), wcol = j0 + wn * 32;   // first row / column of the warp
   // acc[mb][nb8][e]: row = wrow + mb*16 + (e < 2 ? arow0 : arow1),
   //                  col = wcol + colof(nb8, e & 1)
   auto colof = [&](int nb8, int e1) -> int {
@@ -218,7 +251,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   if (P.preload && P.cin != nullptr) {
     if (vec_rows) {
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb)
+      for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
         for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll
@@ -230,7 +263,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
     } else if (vec_cols) {
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb)
+      for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -243,7 +276,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
     } else {
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb)
+      for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
         for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll
@@ -257,14 +290,17 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   }
   for (int kt = 0; kt < KT; ++kt, ++consumed) {
     const int s = (int)(consumed % STAGES);
-    // bounded wait; the give-up decision is made CTA-uniform at the barrier below
-    const bool got = mbar_wait(&full_bar[s], (unsigned)((consumed / STAGES) & 1));
-    if (got) {
+    // bounded wait, its outcome made warp-uniform
+    if (!__all_sync(0xffffffffu, mbar_wait(&full_bar[s], (unsigned)((consumed / STAGES) & 1)))) {
+      ok = false;
+      break;
+    }
+    {
     const unsigned char* As = smem + s * STAGE_BYTES;
     const unsigned char* Bs = As + A_STAGE;
     const int ks = kbase + kt * BK;
     const bool mask_a = TRI && ((P.tri_a == TRI_LOWER && ks + BK - 1 >= wrow) ||
-                                (P.tri_a == TRI_UPPER && ks <= wrow + 63));
+                                (P.tri_a == TRI_UPPER && ks <= wrow + 16 * MB - 1));
     const bool mask_b = TRI && ((P.tri_b == TRI_LOWER && ks + BK - 1 >= wcol) ||
                                 (P.tri_b == TRI_UPPER && ks <= wcol + 31));
 #pragma unroll
@@ -322,10 +358,10 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 #pragma unroll
         for (int s2 = 0; s2 < 2; ++s2) {
           const int k = q * 8 + 2 * t + s2;
-          double2 av[4];
+          double2 av[MB];
 #pragma unroll
-          for (int mb = 0; mb < 4; ++mb) {
-            const unsigned char* box = As + (wm * 4 + mb) * 2048;
+          for (int mb = 0; mb < MB; ++mb) {
+            const unsigned char* box = As + (wm * MB + mb) * 2048;
             av[mb] = *reinterpret_cast<const double2*>(box + k * 128 + ((g ^ (k & 7)) << 4));
             if (mask_a) {
               const int ra = wrow + mb * 16;
@@ -334,7 +370,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             }
           }
 #pragma unroll
-          for (int mb = 0; mb < 4; ++mb)
+          for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
             for (int nb8 = 0; nb8 < 4; ++nb8) {
               double b;
@@ -349,18 +385,18 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         }
       } else {
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb) {
+      for (int mb = 0; mb < MB; ++mb) {
         // A fragments of m16 block mb: av[s2] = (row arow0, row arow1) at step 2q + s2
         double2 av[2];
         if constexpr (LA == LAYOUT_R) {
-          const unsigned char* box = As + (wm * 4 + mb) * 2048;
+          const unsigned char* box = As + (wm * MB + mb) * 2048;
 #pragma unroll
           for (int s2 = 0; s2 < 2; ++s2) {
             const int k = q * 8 + 2 * t + s2;
             av[s2] = *reinterpret_cast<const double2*>(box + k * 128 + ((g ^ (k & 7)) << 4));
           }
         } else {
-          const int r0 = wm * 64 + mb * 16 + fg, r1 = r0 + 8;
+          const int r0 = wm * (16 * MB) + mb * 16 + fg, r1 = r0 + 8;
           const int ch = q * 4 + t;
           const double2 x0 = *reinterpret_cast<const double2*>(As + r0 * 128 + ((ch ^ (r0 & 7)) << 4));
           const double2 x1 = *reinterpret_cast<const double2*>(As + r1 * 128 + ((ch ^ (r1 & 7)) << 4));
@@ -392,17 +428,24 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
       }
     }
       }
-    }   // got
-    // every warp is done with stage s: refill it with k block kt + STAGES
-    if (!__syncthreads_and(got)) {
-      ok = false;
-      break;
     }
-    if (threadIdx.x == 0) produce();
+    // this warp is done with stage s
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty_bar[s]);
+    if (warp == 0) {
+      bool fine = true;
+      if (lane == 0) fine = refill();
+      if (!__shfl_sync(0xffffffffu, fine, 0)) {
+        ok = false;
+        ++consumed;
+        break;
+      }
+    }
   }
   if (!ok) {
-    // a wait gave up: record it, and let thread 0 wait (bounded) for the copies it
-    // issued before the CTA exits
+    // a wait gave up (the other warps' waits then give up too, within their
+    // bounds): record it, and let thread 0 wait (bounded) for the copies it issued
+    // before it exits
     if (lane == 0) atomicExch(P.err, 3);
     if (threadIdx.x == 0)
       for (long long q = consumed; q < issued; ++q) mbar_wait(&full_bar[q % STAGES], (unsigned)((q / STAGES) & 1));
@@ -416,7 +459,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   if (vec_rows) {
     // column-major C: rows arow0 and arow0 + 1 are adjacent
 #pragma unroll
-    for (int mb = 0; mb < 4; ++mb)
+    for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
       for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll
@@ -434,7 +477,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   } else if (vec_cols) {
     // row-contiguous C: the columns of n8 blocks 2p and 2p + 1 are adjacent
 #pragma unroll
-    for (int mb = 0; mb < 4; ++mb)
+    for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
       for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -452,7 +495,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         }
   } else {
 #pragma unroll
-    for (int mb = 0; mb < 4; ++mb)
+    for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
       for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll

@@ -187,32 +187,39 @@ bool make_map(CUtensorMap* map, const double* base, int layout, long long rows, 
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-template <int LA, int LB, bool TRI>
+template <int LA, int LB, bool TRI, int MB>
 CUresult launch_dmma(CULAPACKhandle h, const CUtensorMap& ma, const CUtensorMap& mb, const dmma::Params& q,
                      int tiles, cudaStream_t s, const int* abort) {
+  constexpr int smem = dmma::Shape<MB>::SMEM_BYTES;
   static bool attr = false;
   if (!attr) {
-    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      dmma::SMEM_BYTES));
-    // two CTAs per SM: ask for the whole unified L1/shared carve-out
-    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI>,
+    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+    // several CTAs per SM: ask for the whole unified L1/shared carve-out
+    CUCHOL_CHECK(cudaFuncSetAttribute(dmma::gemm_kernel<LA, LB, TRI, MB>,
                                       cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     attr = true;
   }
-  dmma::gemm_kernel<LA, LB, TRI><<<tiles, dmma::THREADS, dmma::SMEM_BYTES, s>>>(ma, mb, q, abort);
+  dmma::gemm_kernel<LA, LB, TRI, MB><<<tiles, dmma::THREADS, smem, s>>>(ma, mb, q, abort);
   ++h->launches;
   CUCHOL_CHECK(cudaGetLastError());
   return CUDA_SUCCESS;
 }
 
-template <bool TRI>
+template <bool TRI, int MB>
 CUresult launch_dmma_layouts(CULAPACKhandle h, int la, int lb, const CUtensorMap& ma, const CUtensorMap& mb,
                              const dmma::Params& q, int tiles, cudaStream_t s, const int* abort) {
-  if (la == 0 && lb == 0) return launch_dmma<0, 0, TRI>(h, ma, mb, q, tiles, s, abort);
-  if (la == 0 && lb == 1) return launch_dmma<0, 1, TRI>(h, ma, mb, q, tiles, s, abort);
-  if (la == 1 && lb == 0) return launch_dmma<1, 0, TRI>(h, ma, mb, q, tiles, s, abort);
-  return launch_dmma<1, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 0) return launch_dmma<0, 0, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 1) return launch_dmma<0, 1, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  if (la == 1 && lb == 0) return launch_dmma<1, 0, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  return launch_dmma<1, 1, TRI, MB>(h, ma, mb, q, tiles, s, abort);
 }
+
+// Warp tile height of the FP64 engine for a problem (m16 blocks per warp): 64 x 64
+// tiles, three CTAs per SM, for the updates of the factorizations (k up to about a
+// thousand: more resident warps and finer waves measured faster), 128 x 64 tiles,
+// two per SM, for long products (fewer operand bytes per flop).
+inline int dmma_mb(const GemmProblem<double>& p) { return p.k >= 2048 ? 4 : 2; }
 
 // Runs the problem on the FP64 tensor-core engine if its views fit the engine
 // (each view row- or k-contiguous, 16-byte aligned, even leading dimension);
@@ -225,7 +232,8 @@ bool try_dmma(CULAPACKhandle h, const GemmProblem<double>& p, cudaStream_t s, co
   const long long ldb = (lb == dmma::LAYOUT_R) ? p.b_ks : p.b_rs;
   if ((lda & 1) || (ldb & 1) || !aligned16(p.a) || !aligned16(p.b)) return false;
   CUtensorMap ma, mb;
-  if (!make_map(&ma, p.a, la, p.m, p.k, lda, dmma::BM) || !make_map(&mb, p.b, lb, p.n, p.k, ldb, dmma::BN))
+  const int mbk = dmma_mb(p), bm = 32 * mbk;
+  if (!make_map(&ma, p.a, la, p.m, p.k, lda, bm) || !make_map(&mb, p.b, lb, p.n, p.k, ldb, dmma::BN))
     return false;
   dmma::Params q;
   q.c = p.c; q.c_rs = p.c_rs; q.c_cs = p.c_cs;
@@ -242,13 +250,17 @@ bool try_dmma(CULAPACKhandle h, const GemmProblem<double>& p, cudaStream_t s, co
               (p.cin == nullptr || (p.cin_rs == p.c_rs && p.cin_cs == p.c_cs) || p.cin != p.c);
   q.neg = q.preload && p.alpha == -1.0;
   q.err = h->d_words + 3;
-  q.tiles_m = (p.m + dmma::BM - 1) / dmma::BM;
+  q.tiles_m = (p.m + bm - 1) / bm;
   const int all_tiles = q.tiles_m * q.tiles_n;
   // one tile per CTA: several tiles per CTA measured slower (tails, uneven skipping)
   const int tiles = all_tiles;
   const bool tri = p.tri_a || p.tri_b || p.unit_a || p.unit_b;
-  *rc = tri ? launch_dmma_layouts<true>(h, la, lb, ma, mb, q, tiles, s, abort)
-            : launch_dmma_layouts<false>(h, la, lb, ma, mb, q, tiles, s, abort);
+  if (mbk == 2)
+    *rc = tri ? launch_dmma_layouts<true, 2>(h, la, lb, ma, mb, q, tiles, s, abort)
+              : launch_dmma_layouts<false, 2>(h, la, lb, ma, mb, q, tiles, s, abort);
+  else
+    *rc = tri ? launch_dmma_layouts<true, 4>(h, la, lb, ma, mb, q, tiles, s, abort)
+              : launch_dmma_layouts<false, 4>(h, la, lb, ma, mb, q, tiles, s, abort);
   return true;
 }
 

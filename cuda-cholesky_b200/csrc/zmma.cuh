@@ -13,7 +13,9 @@
 // Re and Im: 64 accumulators per thread, as in the real engine).  A stage holds 8
 // complex k of both operands (2 x 8 KB), staged by TMA (cp.async.bulk.tensor.2d,
 // 128-byte swizzle, no multicast) as FP64 pairs into a 4-stage mbarrier ring; two
-// CTAs share an SM.  Thread 0 issues the copies after the CTA-wide release of a stage.
+// CTAs share an SM.  Thread 0 issues the copies; each warp releases a stage on its
+// "empty" mbarrier, and thread 0, after consuming item q, refills the stage of item
+// q - 1 (no CTA-wide barrier in the k loop).
 //
 // Shared memory, one stage and operand (views as in gemm.cuh, complex elements):
 //   layout R (rows contiguous): 8 boxes of 8 complex rows x 8 k; a k-row of a box is
@@ -124,10 +126,14 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) dmma::mbar_init(&full_bar[s], 1);
+    for (int s = 0; s < STAGES; ++s) {
+      dmma::mbar_init(&full_bar[s], 1);
+      dmma::mbar_init(&empty_bar[s], WARPS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -151,9 +157,20 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     ++issued;
     return true;
   };
+  bool more = true;   // thread 0: items are left to issue
   if (threadIdx.x == 0)
-    for (int q = 0; q < STAGES && produce(); ++q) {
+    for (int q = 0; q < STAGES && more; ++q) more = produce();
+  // thread 0, after consuming item `consumed`: issue the items up to consumed - 1 +
+  // STAGES, each into a stage whose previous item every warp has released (bounded
+  // wait); false if a wait gave up
+  auto refill = [&]() -> bool {
+    while (more && issued < consumed + STAGES) {
+      const long long old = issued - STAGES;
+      if (!dmma::mbar_wait(&empty_bar[old % STAGES], (unsigned)((old / STAGES) & 1))) return false;
+      more = produce();
     }
+    return true;
+  };
 
   const int wm = warp & 1, wn = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
@@ -194,8 +211,12 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     }
     for (int kt = 0; kt < KT; ++kt, ++consumed) {
       const int s = (int)(consumed % STAGES);
-      const bool got = dmma::mbar_wait(&full_bar[s], (unsigned)((consumed / STAGES) & 1));
-      if (got) {
+      // bounded wait, its outcome made warp-uniform
+      if (!__all_sync(0xffffffffu, dmma::mbar_wait(&full_bar[s], (unsigned)((consumed / STAGES) & 1)))) {
+        ok = false;
+        break;
+      }
+      {
         const unsigned char* As = smem + s * STAGE_BYTES;
         const unsigned char* Bs = As + A_STAGE;
         const int ks = kbase + kt * BK;
@@ -249,13 +270,22 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             }
         }
       }
-      if (!__syncthreads_and(got)) {
-        ok = false;
-        break;
+      // this warp is done with stage s
+      __syncwarp();
+      if (lane == 0) dmma::mbar_arrive(&empty_bar[s]);
+      if (warp == 0) {
+        bool fine = true;
+        if (lane == 0) fine = refill();
+        if (!__shfl_sync(0xffffffffu, fine, 0)) {
+          ok = false;
+          ++consumed;
+          break;
+        }
       }
-      if (threadIdx.x == 0) produce();
     }
     if (!ok) {
+      // a wait gave up (the other warps' waits then give up too, within their
+      // bounds): record it, and let thread 0 wait (bounded) for the copies it issued
       if (lane == 0) atomicExch(P.err, 3);
       if (threadIdx.x == 0)
         for (long long q = consumed; q < issued; ++q)
