@@ -32,9 +32,10 @@ struct TuneRow {
   int sub;
 };
 
-// FP64 ?potrf, B200: outer blocks of 2 / 3 / 4 / 6 / 8 diagonal blocks, measured at
-// n = 4096 / 8192 / 16384 / 32768 (best 4.25, 11.22, 56.55, 398.1 ms) and split at the
-// geometric midpoints.  C: the rows tune.py wrote from n = 4096 / 8192 / 16384 (best
+// FP64 ?potrf, B200, rows from tune.py with the 64 x 64-tile DMMA updates: outer
+// blocks of 2 / 2 / 5 / 8 diagonal blocks at n = 4096 / 8192 / 16384 / 32768 (best
+// 3.99, 10.78, 54.33, 382.6 ms; at 16384 the other widths gave 57.1 (2), 55.3 (3),
+// 54.8 (4), 54.4 (6), 54.9 (8)), split at the geometric midpoints.  C: the rows tune.py wrote from n = 4096 / 8192 / 16384 (best
 // cpotrf 7.34 / 29.82 / 196.8 ms; outer block 2 gave 208.5 ms at n = 16384).  Z on
 // the complex FP64 tensor-core engine: best 9.93 / 37.56 / 223.9 ms with 2 / 6 / 12
 // (outer block 2 gave 293.5 ms at 16384).  S on the split TF32 tensor-core updates:
@@ -45,8 +46,7 @@ struct TuneRow {
 // 2344 ms at the two larger orders).
 inline std::vector<TuneRow>& tuning_rows() {
   static std::vector<TuneRow> rows = {
-      {TUNE_POTRF, 'D', 0, 2}, {TUNE_POTRF, 'D', 6144, 3}, {TUNE_POTRF, 'D', 12288, 4},
-      {TUNE_POTRF, 'D', 24576, 6}, {TUNE_POTRF, 'D', 49152, 8},
+      {TUNE_POTRF, 'D', 0, 2}, {TUNE_POTRF, 'D', 11585, 5}, {TUNE_POTRF, 'D', 23170, 8},
       {TUNE_POTRF, 'S', 0, 2}, {TUNE_POTRF, 'S', 11585, 4},
       {TUNE_POTRF, 'C', 0, 2}, {TUNE_POTRF, 'C', 5793, 3}, {TUNE_POTRF, 'C', 11585, 6},
       {TUNE_POTRF, 'Z', 0, 2}, {TUNE_POTRF, 'Z', 5793, 6}, {TUNE_POTRF, 'Z', 11585, 12},

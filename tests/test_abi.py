@@ -249,7 +249,7 @@ def test_tuning_table_file(tmp_path):
         assert lib.cuLAPACKGetPotrfBlocks(None, t.encode(), n, C.byref(v)) == 0
         return v.value
 
-    assert sub("D", 1000) == 2 and sub("D", 16384) == 4 and sub("D", 65536) == 8 and sub("Z", 65536) == 12
+    assert sub("D", 1000) == 2 and sub("D", 16384) == 5 and sub("D", 65536) == 8 and sub("Z", 65536) == 12
     rows = tune.table_rows("D", {4096: 2, 8192: 3, 16384: 5})
     assert rows == ["potrf D 0 2", "potrf D 5793 3", "potrf D 11585 5"]
     good = tmp_path / "t.tuning"
@@ -273,7 +273,7 @@ def test_tuning_table_file(tmp_path):
     finally:
         restore = tmp_path / "builtin.tuning"
         lines = ["cucholesky-tuning 1"]
-        lines += ["potrf D 0 2", "potrf D 6144 3", "potrf D 12288 4", "potrf D 24576 6", "potrf D 49152 8",
+        lines += ["potrf D 0 2", "potrf D 11585 5", "potrf D 23170 8",
                   "potrf S 0 2", "potrf S 11585 4", "potrf C 0 2", "potrf C 5793 3",
                   "potrf C 11585 6", "potrf Z 0 2", "potrf Z 5793 6", "potrf Z 11585 12", "ozaki D 0 8", "ozaki D 49152 16"]
         restore.write_text("\n".join(lines) + "\n")

@@ -270,7 +270,7 @@ def test_outer_block_sizes(handle, p, u):
     finally:
         assert lib.cuLAPACKSetPotrfBlocks(handle.value, 0) == 0
     v = C.c_int(0)
-    tune_expected = {"d": 4, "z": 12, "s": 4, "c": 6}
+    tune_expected = {"d": 5, "z": 12, "s": 4, "c": 6}
     assert lib.cuLAPACKGetPotrfBlocks(handle.value, p.upper().encode(), 16384, C.byref(v)) == 0
     assert v.value == tune_expected[p]
 
