@@ -17,8 +17,9 @@ torch Philox on the device, seed = rank) per step.
             with CUDA events on its stream, against the FP64 dense peak measured live
             (best cuBLAS DGEMM 8192^3, with the clocks seen during that probe); its
             DRAM traffic per launch is the ncu-measured bytes per lower-triangle element
-            of C at the same k (dram__bytes_read.sum + dram__bytes_write.sum at m = 8192:
-            14.6 B at k = 256, 16.05 B at k = 512) times the elements, plus the panel once.
+            of C (dram__bytes_read.sum + dram__bytes_write.sum at m = 8192 on the
+            64 x 64-tile kernel: 15.28 B at k = 512; 14.6 B at k = 256 on the earlier
+            128 x 64-tile one) times the elements, plus the panel once.
   cpu_baseline  the reference's own CPU dpotrf (oracle/_ref, compiled from its
             lapack/*.c over blas/*.c, all host cores) on the GPU arm's own matrix at the
             same n = 16384: one untimed and two timed runs.
@@ -367,7 +368,7 @@ def extra_potrf_large(torch, cc, h, peak, n=32768):
     return {"n": n, "potrf_ms": ms, "tflops": tf, "fraction_of_fp64_peak": tf / peak, "outer_block": k,
             "backward_error_n_eps_probe": be, "bound_10": be <= 10,
             "roofline": {"bound": "tensor", "achieved": ktf, "peak": peak, "unit": "TFLOP/s", "frac": ktf / peak,
-                         "kernel": f"dmma::gemm_kernel<0,0,0> SYRK m={n - k} k={k}", "kernel_ms": kms,
+                         "kernel": f"dmma::gemm_kernel<0,0,0,2> SYRK m={n - k} k={k}", "kernel_ms": kms,
                          "algorithmic_flop": kflop}}
 
 
@@ -872,8 +873,9 @@ def run_headline(args, rank, world, local):
     mk = n - kk
     syrk_ms, syrk_tflops, syrk_flops = syrk_roofline(torch, cc, "D", mk, kk, peak)
     # DRAM bytes per lower-triangle element of C measured by ncu on this kernel at
-    # m = 8192 (C read + write): 14.6 at k = 256, 16.05 at k = 512; the panel is read once
-    syrk_traffic = (16.05 if kk >= 512 else 14.6) * (float(mk) * (mk + 1) / 2) + 8.0 * mk * kk
+    # m = 8192 (C read + write): 15.28 at k = 512 (14.6 at k = 256 with 128 x 64
+    # tiles); the panel is read once
+    syrk_traffic = (15.28 if kk >= 512 else 14.6) * (float(mk) * (mk + 1) / 2) + 8.0 * mk * kk
     total_ms = t0.elapsed_time(t1)
     potrf_ms = [a.elapsed_time(b) for a, b in evs]
     if pg:
@@ -973,7 +975,7 @@ def run_headline(args, rank, world, local):
             "backward_error_n_eps_probe": berr,
             "roofline": {"bound": "tensor", "achieved": syrk_tflops, "peak": peak, "unit": "TFLOP/s",
                          "frac": syrk_tflops / peak, "traffic": syrk_traffic,
-                         "kernel": f"dmma::gemm_kernel<0,0,0>: trailing-update SYRK (cuDsyrk L,N) m={mk} k={kk}",
+                         "kernel": f"dmma::gemm_kernel<0,0,0,2> (64 x 64 tiles): trailing-update SYRK (cuDsyrk L,N) m={mk} k={kk}",
                          "kernel_ms": syrk_ms, "algorithmic_flop": syrk_flops,
                          "algorithmic_bytes": 16.0 * (float(mk) * (mk + 1) / 2) + 8.0 * mk * kk,
                          "peak_source": "FP64 dense peak measured live: best cuBLAS DGEMM 8192^3 on this GPU",
