@@ -286,31 +286,39 @@ bool make_zmap(CUtensorMap* map, const cuDoubleComplex* base, int layout, long l
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int LA, int LB, bool TRI>
+template <int LA, int LB, bool TRI, int MB>
 CUresult launch_zmma(CULAPACKhandle h, const CUtensorMap& ma, const CUtensorMap& mb, const zmma::Params& q,
                      int tiles, cudaStream_t s, const int* abort) {
+  constexpr int smem = zmma::Shape<MB>::SMEM_BYTES;
   static bool attr = false;
   if (!attr) {
-    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      zmma::SMEM_BYTES));
-    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI>,
+    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+    CUCHOL_CHECK(cudaFuncSetAttribute(zmma::gemm_kernel<LA, LB, TRI, MB>,
                                       cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     attr = true;
   }
-  zmma::gemm_kernel<LA, LB, TRI><<<tiles, zmma::THREADS, zmma::SMEM_BYTES, s>>>(ma, mb, q, abort);
+  zmma::gemm_kernel<LA, LB, TRI, MB><<<tiles, zmma::THREADS, smem, s>>>(ma, mb, q, abort);
   ++h->launches;
   CUCHOL_CHECK(cudaGetLastError());
   return CUDA_SUCCESS;
 }
 
-template <bool TRI>
+template <bool TRI, int MB>
 CUresult launch_zmma_layouts(CULAPACKhandle h, int la, int lb, const CUtensorMap& ma, const CUtensorMap& mb,
                              const zmma::Params& q, int tiles, cudaStream_t s, const int* abort) {
-  if (la == 0 && lb == 0) return launch_zmma<0, 0, TRI>(h, ma, mb, q, tiles, s, abort);
-  if (la == 0 && lb == 1) return launch_zmma<0, 1, TRI>(h, ma, mb, q, tiles, s, abort);
-  if (la == 1 && lb == 0) return launch_zmma<1, 0, TRI>(h, ma, mb, q, tiles, s, abort);
-  return launch_zmma<1, 1, TRI>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 0) return launch_zmma<0, 0, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  if (la == 0 && lb == 1) return launch_zmma<0, 1, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  if (la == 1 && lb == 0) return launch_zmma<1, 0, TRI, MB>(h, ma, mb, q, tiles, s, abort);
+  return launch_zmma<1, 1, TRI, MB>(h, ma, mb, q, tiles, s, abort);
 }
+
+// Warp tile height of the complex engine for a problem (m16 blocks per warp): 32 x 64
+// tiles, three CTAs per SM, for k < 1024 (the updates of zpotrf up to n = 16384: their
+// CTAs retire twice as often, so the panel chain finds SMs sooner; zpotrf n = 8192
+// 38.2 -> 36.9 ms, n = 4096 9.7 -> 8.7 ms), 64 x 64 otherwise.
+constexpr int kZmmaShortK = 1024;
+inline int zmma_mb(const GemmProblem<cuDoubleComplex>& p) { return p.k < kZmmaShortK ? 1 : 2; }
 
 // Runs a complex double problem on the FP64 tensor-core engine when both operand
 // views are row- or k-contiguous and 16-byte aligned; false (nothing launched)
@@ -324,7 +332,8 @@ bool try_zmma(CULAPACKhandle h, const GemmProblem<cuDoubleComplex>& p, cudaStrea
   const long long ldb = (lb == dmma::LAYOUT_R) ? p.b_ks : p.b_rs;
   if (!aligned16(p.a) || !aligned16(p.b)) return false;
   CUtensorMap ma, mb;
-  if (!make_zmap(&ma, p.a, la, p.m, p.k, lda, zmma::BM) || !make_zmap(&mb, p.b, lb, p.n, p.k, ldb, zmma::BN))
+  const int mbk = zmma_mb(p), bm = 32 * mbk;
+  if (!make_zmap(&ma, p.a, la, p.m, p.k, lda, bm) || !make_zmap(&mb, p.b, lb, p.n, p.k, ldb, zmma::BN))
     return false;
   zmma::Params q;
   q.c = p.c; q.c_rs = p.c_rs; q.c_cs = p.c_cs;
@@ -334,7 +343,7 @@ bool try_zmma(CULAPACKhandle h, const GemmProblem<cuDoubleComplex>& p, cudaStrea
   q.conj_a = p.conj_a; q.conj_b = p.conj_b;
   q.tri_a = p.tri_a; q.tri_b = p.tri_b; q.unit_a = p.unit_a; q.unit_b = p.unit_b;
   q.lower_only = p.lower_only; q.real_diag = p.real_diag;
-  q.tiles_m = (p.m + zmma::BM - 1) / zmma::BM;
+  q.tiles_m = (p.m + bm - 1) / bm;
   q.tiles_n = (p.n + zmma::BN - 1) / zmma::BN;
   const bool unit_alpha = p.alpha.y == 0.0 && (p.alpha.x == 1.0 || p.alpha.x == -1.0);
   q.preload = unit_alpha &&
@@ -343,8 +352,12 @@ bool try_zmma(CULAPACKhandle h, const GemmProblem<cuDoubleComplex>& p, cudaStrea
   q.err = h->d_words + 3;
   const int tiles = q.tiles_m * q.tiles_n;
   const bool tri = p.tri_a || p.tri_b || p.unit_a || p.unit_b;
-  *rc = tri ? launch_zmma_layouts<true>(h, la, lb, ma, mb, q, tiles, s, abort)
-            : launch_zmma_layouts<false>(h, la, lb, ma, mb, q, tiles, s, abort);
+  if (mbk == 1)
+    *rc = tri ? launch_zmma_layouts<true, 1>(h, la, lb, ma, mb, q, tiles, s, abort)
+              : launch_zmma_layouts<false, 1>(h, la, lb, ma, mb, q, tiles, s, abort);
+  else
+    *rc = tri ? launch_zmma_layouts<true, 2>(h, la, lb, ma, mb, q, tiles, s, abort)
+              : launch_zmma_layouts<false, 2>(h, la, lb, ma, mb, q, tiles, s, abort);
   return true;
 }
 

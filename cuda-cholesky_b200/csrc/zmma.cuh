@@ -10,7 +10,8 @@
 // plain accumulate.  Each output keeps two FP64 accumulators (Re, Im).
 //
 // Tiles: 64 x 64 complex outputs per CTA, four warps of 32 x 32 (2 m16 x 4 n8 blocks,
-// Re and Im: 64 accumulators per thread, as in the real engine).  A stage holds 8
+// Re and Im: 64 accumulators per thread, as in the real engine), or, for products with
+// k < 1024, 32 x 64 with warps of 16 x 32 (three CTAs per SM).  A stage holds 8
 // complex k of both operands (2 x 8 KB), staged by TMA (cp.async.bulk.tensor.2d,
 // 128-byte swizzle, no multicast) as FP64 pairs into a 4-stage mbarrier ring; two
 // CTAs share an SM.  Thread 0 issues the copies; each warp releases a stage on its
@@ -36,13 +37,22 @@
 namespace cuchol {
 namespace zmma {
 
-constexpr int BM = 64, BN = 64, BK = 8, STAGES = 4;      // complex elements
-constexpr int WARPS = 4;                                  // 2 x 2 warps of 32 x 32
+constexpr int BN = 64, BK = 8;                            // complex elements
+constexpr int WARPS = 4;                                  // 2 x 2 warps of (16 MB) x 32
 constexpr int THREADS = WARPS * 32;
-constexpr int A_STAGE = BM * BK * 16;                     // 8 KB
 constexpr int B_STAGE = BN * BK * 16;                     // 8 KB
-constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
+
+// A tile shape: MB m16 blocks per warp, BM = 32 MB rows per CTA (MB = 2: 64 x 64 tiles,
+// two CTAs per SM; MB = 1: 32 x 64 tiles, half the accumulators, three CTAs per SM).
+template <int MB>
+struct Shape {
+  static constexpr int BM = 32 * MB;
+  static constexpr int STAGES = 4;
+  static constexpr int MIN_CTAS = MB == 2 ? 2 : 3;
+  static constexpr int A_STAGE = BM * BK * 16;            // 8 KB (MB = 2) or 4 KB
+  static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB alignment slack
+};
 constexpr int BOX = 1024;                                 // layout R box: 8 rows x 8 k
 
 using dmma::LAYOUT_K;
@@ -102,10 +112,12 @@ __device__ __forceinline__ cuDoubleComplex cmul(cuDoubleComplex a, cuDoubleCompl
   return make_cuDoubleComplex(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 
-template <int LA, int LB, bool TRI>
-__global__ void __launch_bounds__(THREADS, 2)
+template <int LA, int LB, bool TRI, int MB>
+__global__ void __launch_bounds__(THREADS, Shape<MB>::MIN_CTAS)
 gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             const __grid_constant__ Params P, const int* __restrict__ abort_flag) {
+  constexpr int BM = Shape<MB>::BM, STAGES = Shape<MB>::STAGES;
+  constexpr int A_STAGE = Shape<MB>::A_STAGE, STAGE_BYTES = Shape<MB>::STAGE_BYTES;
   if (cta_aborted(abort_flag)) return;
   const int ntiles = P.tiles_m * P.tiles_n;
   auto tile_range = [&](int tile, int& i0, int& j0, int& kbase, int& KT) -> bool {
@@ -185,17 +197,17 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     if (!tile_range(tile, i0, j0, kbase, KT)) continue;
     // acc[mb][nb8][e]: Re (accr) and Im (acci) of row wrow + mb*16 + g (+8 for e >= 2),
     // column wcol + nb8*8 + 2t + (e & 1)
-    double accr[2][4][4], acci[2][4][4];
+    double accr[MB][4][4], acci[MB][4][4];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < MB; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
         for (int c = 0; c < 4; ++c) accr[a][b][c] = acci[a][b][c] = 0.0;
-    const int wrow = i0 + wm * 32, wcol = j0 + wn * 32;
+    const int wrow = i0 + wm * (16 * MB), wcol = j0 + wn * 32;
     if (P.preload && P.cin != nullptr) {
 #pragma unroll
-      for (int mb = 0; mb < 2; ++mb)
+      for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
         for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll
@@ -222,7 +234,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         const int ks = kbase + kt * BK;
         // k blocks that reach the diagonal of a triangular view (its unit diagonal too)
         const bool mask_a = TRI && ((P.tri_a == TRI_LOWER && ks + BK - 1 >= wrow) ||
-                                    (P.tri_a == TRI_UPPER && ks <= wrow + 31));
+                                    (P.tri_a == TRI_UPPER && ks <= wrow + 16 * MB - 1));
         const bool mask_b = TRI && ((P.tri_b == TRI_LOWER && ks + BK - 1 >= wcol) ||
                                     (P.tri_b == TRI_UPPER && ks <= wcol + 31));
 #pragma unroll
@@ -240,10 +252,10 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
             nbi[nb8] = flip(v.y, m_bi ^ SIGN);
           }
           // A fragments: rows g and g + 8 of each m16 block (Re a, Im a')
-          double ar[2][2], ai[2][2];
+          double ar[MB][2], ai[MB][2];
 #pragma unroll
-          for (int mb = 0; mb < 2; ++mb) {
-            const int r0 = wm * 32 + mb * 16 + g;
+          for (int mb = 0; mb < MB; ++mb) {
+            const int r0 = wm * (16 * MB) + mb * 16 + g;
             double2 a0 = frag<LA>(As, r0, k), a1 = frag<LA>(As, r0 + 8, k);
             if (mask_a) {
               a0 = tri_mask(a0, P.tri_a, P.unit_a, i0 + r0, ks + k);
@@ -255,14 +267,14 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           // 16 independent accumulator chains; each chain's two MMAs of this step are
           // 16 MMAs apart
 #pragma unroll
-          for (int mb = 0; mb < 2; ++mb)
+          for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
             for (int nb8 = 0; nb8 < 4; ++nb8) {
               dmma::dmma_16x8x4(accr[mb][nb8], ar[mb][0], ar[mb][1], br[nb8]);
               dmma::dmma_16x8x4(acci[mb][nb8], ar[mb][0], ar[mb][1], bi[nb8]);
             }
 #pragma unroll
-          for (int mb = 0; mb < 2; ++mb)
+          for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
             for (int nb8 = 0; nb8 < 4; ++nb8) {
               dmma::dmma_16x8x4(accr[mb][nb8], ai[mb][0], ai[mb][1], nbi[nb8]);
@@ -296,7 +308,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     // epilogue: preload -> C = acc; else C = alpha * acc + beta * Cin
     const bool has_cin = (P.cin != nullptr) && !P.preload;
 #pragma unroll
-    for (int mb = 0; mb < 2; ++mb)
+    for (int mb = 0; mb < MB; ++mb)
 #pragma unroll
       for (int nb8 = 0; nb8 < 4; ++nb8)
 #pragma unroll
